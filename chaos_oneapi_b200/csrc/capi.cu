@@ -1,0 +1,509 @@
+// C ABI of the sweep (include/chaos_lyap.h): model registry, handles,
+// argument checking, launch dispatch, host-buffer path, autotuner and the
+// drop-in for the reference launcher cudaLyapunov.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/chaos_lyap.h"
+#include "kernels.h"
+#include "models.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(CHAOS_LYAP_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+struct ModelInfo {
+  const char *name;
+  int id, dim, nparams, type;
+  const char *pnames, *phase, *eq;
+};
+
+// The registry the reference fills at static-initialisation time
+// (model_factory.h:36-39, shimizu.dp.cpp:203-204); here the device code is
+// compiled in (models.cuh) and the table only carries the descriptions.
+const ModelInfo kModels[] = {
+    {"chua", chaos::kChua, 3, 4, 0, "alpha, beta, m0, m1", "x, y, z",
+     "x' = alpha * (y - x - f(x));y' = x - y + z;z' = - beta * y;"
+     "f(x) = m1 * x + 0.5 * (m0 - m1) * (|x + 1| - |x - 1|)"},
+    {"hyper_rossler", chaos::kHyperRossler, 4, 2, 0, "c, d", "x, y, z, w",
+     "x' = - y - z;y' = x + 0.25 * y + w;z' = 3 + x * z;w' = - c * z + d * w"},
+    {"lorenz", chaos::kLorenz, 3, 3, 0, "sigma, rho, beta", "x, y, z",
+     "x' = sigma * (y - x);y' = x * (rho - z) - y;z' = x * y - beta * z"},
+    {"lorenz96", chaos::kLorenz96, 40, 2, 0, "F, gamma", "x0..x39",
+     "x_i' = (x_{i+1} - x_{i-2}) * x_{i-1} - gamma * x_i + F (cyclic, N = 40)"},
+    {"rossler", chaos::kRossler, 3, 3, 0, "a, b, c", "x, y, z",
+     "x' = - y - z;y' = x + a * y;z' = b + z * (x - c)"},
+    {"shimizu", chaos::kShimizu, 3, 2, 0, "alpha, lamda", "x, y, z",
+     "x' = y;y' = - alpha * y - x * z + x;z' = - lamda * z + x ** 2.0"},
+};
+constexpr int kModelCount = sizeof(kModels) / sizeof(kModels[0]);
+
+const ModelInfo *find_model(const char *name) {
+  if (!name) return nullptr;
+  for (const auto &m : kModels)
+    if (std::strcmp(m.name, name) == 0) return &m;
+  return nullptr;
+}
+
+// Keeps the caller's current device across a call.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    ok = (prev == dev) || cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+chaos::View view(double *p, int64_t P, int C, int layout) {
+  return layout == CHAOS_LAYOUT_COMP_MAJOR ? chaos::View{p, 1, P} : chaos::View{p, C, 1};
+}
+chaos::CView cview(const double *p, int64_t P, int C, int layout) {
+  return layout == CHAOS_LAYOUT_COMP_MAJOR ? chaos::CView{p, 1, P} : chaos::CView{p, C, 1};
+}
+
+}  // namespace
+
+struct chaos_lyap_handle {
+  chaos_lyap_desc d;
+  const ModelInfo *model;
+  int sm_count = 0;
+  int block = 0;
+  int schedule = CHAOS_SCHED_PERSISTENT;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t last_stream = nullptr;
+  unsigned long long *queue = nullptr;  // persistent-schedule point counter
+  // host-path staging
+  double *s_params = nullptr, *s_inits = nullptr, *s_spec = nullptr, *s_tavg = nullptr;
+  int32_t *s_status = nullptr;
+  int64_t *s_steps = nullptr;
+  int64_t s_cap = 0;
+};
+
+extern "C" {
+
+int chaos_lyap_abi_version(void) { return CHAOS_LYAP_ABI_VERSION; }
+
+const char *chaos_lyap_last_error(void) { return g_err.c_str(); }
+
+int chaos_lyap_desc_init(chaos_lyap_desc *d) {
+  if (!d) return fail(CHAOS_LYAP_EINVAL, "desc is null");
+  std::memset(d, 0, sizeof *d);
+  d->struct_size = (int32_t)sizeof *d;
+  std::strcpy(d->model, "lorenz");
+  d->method = CHAOS_METHOD_VAR;
+  d->integrator = CHAOS_INTEG_DVERK65;
+  d->precision = CHAOS_PREC_FP64;
+  d->gs = CHAOS_GS_CLASSICAL;
+  d->layout = CHAOS_LAYOUT_POINT_MAJOR;
+  d->eps = 1e-7;
+  d->h = 1e-3;
+  d->rtol = d->atol = 1e-10;
+  d->max_steps = 100000000LL;
+  d->escape = 1e8;
+  d->schedule = CHAOS_SCHED_AUTO;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_model_count(void) { return kModelCount; }
+
+int chaos_lyap_model_name(int index, char *buf, int buflen) {
+  if (index < 0 || index >= kModelCount || !buf || buflen <= 0)
+    return fail(CHAOS_LYAP_EINVAL, "model index %d out of range", index);
+  std::snprintf(buf, (size_t)buflen, "%s", kModels[index].name);
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_query_model(const char *name, int32_t *dim, int32_t *nparams, int32_t *type) {
+  const ModelInfo *m = find_model(name);
+  if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", name ? name : "(null)");
+  if (dim) *dim = m->dim;
+  if (nparams) *nparams = m->nparams;
+  if (type) *type = m->type;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_model_text(const char *name, int which, char *buf, int buflen) {
+  const ModelInfo *m = find_model(name);
+  if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", name ? name : "(null)");
+  if (!buf || buflen <= 0 || which < 0 || which > 2) return fail(CHAOS_LYAP_EINVAL, "bad buffer");
+  const char *s = which == 0 ? m->pnames : which == 1 ? m->phase : m->eq;
+  std::snprintf(buf, (size_t)buflen, "%s", s);
+  return (int)std::strlen(s) < buflen ? CHAOS_LYAP_OK
+                                      : fail(CHAOS_LYAP_EINVAL, "buffer too small");
+}
+
+static int check_desc(const chaos_lyap_desc *d, const ModelInfo **mout) {
+  if (!d) return fail(CHAOS_LYAP_EINVAL, "desc is null");
+  if (d->struct_size != (int32_t)sizeof(chaos_lyap_desc))
+    return fail(CHAOS_LYAP_EINVAL, "desc.struct_size %d != %d", d->struct_size,
+                (int)sizeof(chaos_lyap_desc));
+  char name[33];
+  std::memcpy(name, d->model, 32);
+  name[32] = 0;
+  const ModelInfo *m = find_model(name);
+  if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", name);
+  *mout = m;
+  if (d->k < 1 || d->k > m->dim)
+    return fail(CHAOS_LYAP_EINVAL, "k = %d outside 1..%d for model %s", d->k, m->dim, m->name);
+  if (d->layout != CHAOS_LAYOUT_POINT_MAJOR && d->layout != CHAOS_LAYOUT_COMP_MAJOR)
+    return fail(CHAOS_LYAP_EINVAL, "bad layout %d", d->layout);
+  if (d->method < CHAOS_METHOD_FD || d->method > CHAOS_METHOD_QR)
+    return fail(CHAOS_LYAP_EINVAL, "bad method %d", d->method);
+  if (!(d->h > 0) || !std::isfinite(d->h)) return fail(CHAOS_LYAP_EINVAL, "h must be > 0");
+  if (d->precision == CHAOS_PREC_COMPAT_FP64) {
+    if (d->integrator != CHAOS_INTEG_DVERK_FIXED)
+      return fail(CHAOS_LYAP_EINVAL, "compat precision needs the fixed-step DVERK integrator");
+    if (d->method == CHAOS_METHOD_QR && d->k != m->dim)
+      return fail(CHAOS_LYAP_EUNSUPPORTED,
+                  "QR method needs k == dim (the reference's QR assumes a square matrix)");
+    if (!(d->t_avg > 0)) return fail(CHAOS_LYAP_EINVAL, "t_avg must be > 0");
+  } else if (d->precision == CHAOS_PREC_FP64 || d->precision == CHAOS_PREC_FP32) {
+    if (d->integrator != CHAOS_INTEG_DVERK65 && d->integrator != CHAOS_INTEG_DOPRI5)
+      return fail(CHAOS_LYAP_EINVAL, "adaptive precision forms need DVERK65 or DOPRI5");
+    if (d->method != CHAOS_METHOD_VAR)
+      return fail(CHAOS_LYAP_EUNSUPPORTED, "adaptive forms integrate the variational equations (VAR)");
+    if (d->k != m->dim && m->dim <= 4)
+      return fail(CHAOS_LYAP_EUNSUPPORTED, "adaptive forms compute the full spectrum (k == dim)");
+    if (!(d->rtol > 0) || !(d->atol > 0)) return fail(CHAOS_LYAP_EINVAL, "rtol/atol must be > 0");
+    if (!(d->dt_renorm > 0) || !(d->t_avg > 0) || d->t_transient < 0 || d->t_align < 0)
+      return fail(CHAOS_LYAP_EINVAL, "times: dt_renorm, t_avg > 0; t_transient, t_align >= 0");
+    if (d->max_steps <= 0) return fail(CHAOS_LYAP_EINVAL, "max_steps must be > 0");
+    if (d->gs != CHAOS_GS_CLASSICAL && d->gs != CHAOS_GS_MODIFIED)
+      return fail(CHAOS_LYAP_EINVAL, "bad gs %d", d->gs);
+  } else {
+    return fail(CHAOS_LYAP_EINVAL, "bad precision %d", d->precision);
+  }
+  if (m->type != 0) return fail(CHAOS_LYAP_EUNSUPPORTED, "map models are not provided");
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_create(const chaos_lyap_desc *desc, chaos_lyap_handle **out) {
+  if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
+  *out = nullptr;
+  chaos_lyap_desc d;
+  if (!desc) return fail(CHAOS_LYAP_EINVAL, "desc is null");
+  d = *desc;
+  const ModelInfo *m0 = find_model(d.model);
+  if (d.k == 0 && m0) d.k = m0->dim;
+  const ModelInfo *m = nullptr;
+  int rc = check_desc(&d, &m);
+  if (rc) return rc;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  if (d.device < 0 || d.device >= ndev)
+    return fail(CHAOS_LYAP_EINVAL, "device %d not present (%d devices)", d.device, ndev);
+  DeviceGuard g(d.device);
+  if (!g.ok) return fail(CHAOS_LYAP_ECUDA, "cannot select device %d", d.device);
+  auto *h = new chaos_lyap_handle();
+  h->d = d;
+  h->model = m;
+  cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, d.device);
+  h->block = d.block > 0 ? d.block : (d.precision == CHAOS_PREC_COMPAT_FP64 ? 64 : 128);
+  h->schedule = d.schedule == CHAOS_SCHED_DIRECT ? CHAOS_SCHED_DIRECT : CHAOS_SCHED_PERSISTENT;
+  if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete h;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  if ((e = cudaMalloc(&h->queue, sizeof(unsigned long long))) != cudaSuccess) {
+    cudaStreamDestroy(h->own_stream);
+    delete h;
+    return fail(CHAOS_LYAP_ENOMEM, "cudaMalloc(queue): %s", cudaGetErrorString(e));
+  }
+  *out = h;
+  return CHAOS_LYAP_OK;
+}
+
+static void free_staging(chaos_lyap_handle *h) {
+  cudaFree(h->s_params);
+  cudaFree(h->s_inits);
+  cudaFree(h->s_spec);
+  cudaFree(h->s_tavg);
+  cudaFree(h->s_status);
+  cudaFree(h->s_steps);
+  h->s_params = h->s_inits = h->s_spec = h->s_tavg = nullptr;
+  h->s_status = nullptr;
+  h->s_steps = nullptr;
+  h->s_cap = 0;
+}
+
+int chaos_lyap_destroy(chaos_lyap_handle *h) {
+  if (!h) return CHAOS_LYAP_OK;
+  DeviceGuard g(h->d.device);
+  cudaStreamSynchronize(h->own_stream);
+  free_staging(h);
+  cudaFree(h->queue);
+  cudaStreamDestroy(h->own_stream);
+  delete h;
+  return CHAOS_LYAP_OK;
+}
+
+static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double *inits,
+                   double *spectrum, int32_t *status, int64_t *steps, const double *tavg,
+                   cudaStream_t s, int block, int schedule, double t_avg_override,
+                   double t_transient_override) {
+  const chaos_lyap_desc &d = h->d;
+  const ModelInfo *m = h->model;
+  int rc;
+  if (d.precision == CHAOS_PREC_COMPAT_FP64) {
+    chaos::CompatArgs a{};
+    a.P = P;
+    a.k = d.k;
+    a.method = d.method;
+    a.eps = d.eps;
+    a.step = d.h;
+    a.t_skip = d.t_transient;
+    a.t_skip_clp = d.t_align;
+    a.calc_time = d.t_avg;
+    a.add_skip = d.dt_renorm / d.h;  // tasklyapunov.cpp:65
+    a.params = cview(params, P, m->nparams, d.layout);
+    a.inits = view(inits, P, m->dim, d.layout);
+    a.close = nullptr;
+    a.lyap = view(spectrum, P, d.k, d.layout);
+    a.accumulate = 0;
+    a.status = status;
+    rc = chaos::launch_compat(m->id, a, block, s);
+  } else {
+    chaos::AdaptiveArgs a{};
+    a.P = P;
+    a.k = d.k;
+    a.gs = d.gs;
+    a.rtol = d.rtol;
+    a.atol = d.atol;
+    a.h0 = d.h;
+    a.hmax = d.h_max;
+    a.hmin = d.h_min;
+    a.t_transient = t_transient_override >= 0 ? t_transient_override : d.t_transient;
+    a.t_align = d.t_align;
+    a.t_avg = t_avg_override > 0 ? t_avg_override : d.t_avg;
+    a.dt_renorm = d.dt_renorm;
+    a.max_steps = d.max_steps;
+    a.escape = d.escape > 0 ? d.escape : 1e8;
+    a.params = cview(params, P, m->nparams, d.layout);
+    a.inits = cview(inits, P, m->dim, d.layout);
+    a.t_avg_per_point = t_avg_override > 0 ? nullptr : tavg;
+    a.spectrum = view(spectrum, P, d.k, d.layout);
+    a.status = status;
+    a.steps = steps;
+    const int integ = d.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
+    const int prec = d.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
+    if (m->dim > 4) {
+      rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
+    } else if (schedule == CHAOS_SCHED_PERSISTENT) {
+      cudaError_t e = cudaMemsetAsync(h->queue, 0, sizeof(unsigned long long), s);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
+      a.queue = h->queue;
+      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);
+    } else {
+      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);
+    }
+  }
+  if (rc == chaos::kErrUnsupported)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "no kernel for model %s with this integrator/precision/k",
+                m->name);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "kernel launch");
+  h->last_stream = s;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_run(chaos_lyap_handle *h, int64_t P, const double *params, double *inits,
+                   double *spectrum, int32_t *status, int64_t *steps, const double *tavg,
+                   void *stream) {
+  if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
+  if (P < 0) return fail(CHAOS_LYAP_EINVAL, "P < 0");
+  if (P == 0) return CHAOS_LYAP_OK;
+  if (!params || !inits || !spectrum) return fail(CHAOS_LYAP_EINVAL, "null array");
+  DeviceGuard g(h->d.device);
+  if (!g.ok) return fail(CHAOS_LYAP_ECUDA, "cannot select device %d", h->d.device);
+  return enqueue(h, P, params, inits, spectrum, status, steps, tavg, (cudaStream_t)stream, h->block,
+                 h->schedule, -1.0, -1.0);
+}
+
+int chaos_lyap_sync(chaos_lyap_handle *h) {
+  if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
+  DeviceGuard g(h->d.device);
+  cudaError_t e = h->last_stream ? cudaStreamSynchronize(h->last_stream) : cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "sweep");
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_run_host(chaos_lyap_handle *h, int64_t P, const double *params, double *inits,
+                        double *spectrum, int32_t *status, int64_t *steps, const double *tavg) {
+  if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
+  if (P < 0) return fail(CHAOS_LYAP_EINVAL, "P < 0");
+  if (P == 0) return CHAOS_LYAP_OK;
+  if (!params || !inits || !spectrum) return fail(CHAOS_LYAP_EINVAL, "null array");
+  DeviceGuard g(h->d.device);
+  if (!g.ok) return fail(CHAOS_LYAP_ECUDA, "cannot select device %d", h->d.device);
+  const ModelInfo *m = h->model;
+  const int k = h->d.k;
+  cudaError_t e;
+  if (P > h->s_cap) {
+    free_staging(h);
+    if ((e = cudaMalloc(&h->s_params, sizeof(double) * P * m->nparams)) != cudaSuccess ||
+        (e = cudaMalloc(&h->s_inits, sizeof(double) * P * m->dim)) != cudaSuccess ||
+        (e = cudaMalloc(&h->s_spec, sizeof(double) * P * k)) != cudaSuccess ||
+        (e = cudaMalloc(&h->s_tavg, sizeof(double) * P)) != cudaSuccess ||
+        (e = cudaMalloc(&h->s_status, sizeof(int32_t) * P)) != cudaSuccess ||
+        (e = cudaMalloc(&h->s_steps, sizeof(int64_t) * P)) != cudaSuccess) {
+      free_staging(h);
+      return fail(CHAOS_LYAP_ENOMEM, "staging for %lld points: %s", (long long)P,
+                  cudaGetErrorString(e));
+    }
+    h->s_cap = P;
+  }
+  cudaStream_t s = h->own_stream;
+  const size_t bp = sizeof(double) * P * m->nparams, bx = sizeof(double) * P * m->dim,
+               bs = sizeof(double) * P * k;
+  if ((e = cudaMemcpyAsync(h->s_params, params, bp, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(h->s_inits, inits, bx, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e, "copy in");
+  if (tavg && (e = cudaMemcpyAsync(h->s_tavg, tavg, sizeof(double) * P, cudaMemcpyHostToDevice,
+                                   s)) != cudaSuccess)
+    return cuda_fail(e, "copy in");
+  int rc = enqueue(h, P, h->s_params, h->s_inits, h->s_spec, status ? h->s_status : nullptr,
+                   steps ? h->s_steps : nullptr, tavg ? h->s_tavg : nullptr, s, h->block,
+                   h->schedule, -1.0, -1.0);
+  if (rc) return rc;
+  if ((e = cudaMemcpyAsync(spectrum, h->s_spec, bs, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "copy out");
+  if (h->d.precision == CHAOS_PREC_COMPAT_FP64 &&
+      (e = cudaMemcpyAsync(inits, h->s_inits, bx, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "copy out");
+  if (status && (e = cudaMemcpyAsync(status, h->s_status, sizeof(int32_t) * P,
+                                     cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "copy out");
+  if (steps && (e = cudaMemcpyAsync(steps, h->s_steps, sizeof(int64_t) * P,
+                                    cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "copy out");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "synchronize");
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
+                        const double *inits, int32_t *block_out, int32_t *schedule_out) {
+  if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
+  if (sample <= 0 || !params || !inits) return fail(CHAOS_LYAP_EINVAL, "bad sample");
+  if (h->d.precision == CHAOS_PREC_COMPAT_FP64 || h->model->dim > 4) {
+    if (block_out) *block_out = h->block;
+    if (schedule_out) *schedule_out = h->schedule;
+    return CHAOS_LYAP_OK;
+  }
+  DeviceGuard g(h->d.device);
+  const int k = h->d.k;
+  double *spec = nullptr;
+  cudaError_t e;
+  if ((e = cudaMalloc(&spec, sizeof(double) * sample * k)) != cudaSuccess)
+    return fail(CHAOS_LYAP_ENOMEM, "autotune buffer: %s", cudaGetErrorString(e));
+  // Short horizons: the launch-shape ranking does not need the full run.
+  const double t_avg = std::min(h->d.t_avg, 20.0 * h->d.dt_renorm);
+  const double t_tr = std::min(h->d.t_transient, 5.0 * h->d.dt_renorm);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks[] = {32, 64, 128};
+  const int scheds[] = {CHAOS_SCHED_DIRECT, CHAOS_SCHED_PERSISTENT};
+  float best = 1e30f;
+  int best_b = h->block, best_s = h->schedule, rc = CHAOS_LYAP_OK;
+  cudaStream_t s = h->own_stream;
+  for (int b : blocks)
+    for (int sc : scheds) {
+      float ms = 0;
+      for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
+        cudaEventRecord(e0, s);
+        rc = enqueue(h, sample, params, const_cast<double *>(inits), spec, nullptr, nullptr,
+                     nullptr, s, b, sc, t_avg, t_tr);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);  // second repetition is the warm one
+      }
+      if (rc) break;
+      if (ms < best) {
+        best = ms;
+        best_b = b;
+        best_s = sc;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(spec);
+  if (rc) return rc;
+  h->block = best_b;
+  h->schedule = best_s;
+  if (block_out) *block_out = best_b;
+  if (schedule_out) *schedule_out = best_s;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_cudaLyapunov(int bn, int bs, size_t taskNum, int isQr, int isVar, int modelType,
+                            double *inits, double *closePoints, int32_t dimension,
+                            const char *model, double *params, int32_t paramsDim, double eps,
+                            double integrationStep, double *lyapExps, int32_t expsNum,
+                            double timeSkip, double timeSkipClP, double calcTime,
+                            double addSkipSteps, void *stream) {
+  (void)bn;
+  (void)bs;
+  const ModelInfo *m = find_model(model);
+  if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", model ? model : "(null)");
+  if (modelType != 0 || m->type != 0)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "map models are not provided");
+  if (dimension != m->dim || paramsDim != m->nparams)
+    return fail(CHAOS_LYAP_EINVAL, "model %s has dim %d and %d params (got %d, %d)", m->name,
+                m->dim, m->nparams, dimension, paramsDim);
+  if (expsNum < 1 || expsNum > m->dim) return fail(CHAOS_LYAP_EINVAL, "expsNum out of range");
+  if (isQr && expsNum != m->dim)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "QR method needs expsNum == dimension");
+  if (!(integrationStep > 0)) return fail(CHAOS_LYAP_EINVAL, "integrationStep must be > 0");
+  if (taskNum == 0) return CHAOS_LYAP_OK;
+  if (!inits || !params || !lyapExps) return fail(CHAOS_LYAP_EINVAL, "null array");
+  chaos::CompatArgs a{};
+  a.P = (int64_t)taskNum;
+  a.k = expsNum;
+  a.method = isQr ? 2 : (isVar ? 1 : 0);
+  a.eps = eps;
+  a.step = integrationStep;
+  a.t_skip = timeSkip;
+  a.t_skip_clp = timeSkipClP;
+  a.calc_time = calcTime;
+  a.add_skip = addSkipSteps;
+  a.params = chaos::CView{params, paramsDim, 1};
+  a.inits = chaos::View{inits, dimension, 1};
+  a.close = closePoints;
+  a.lyap = chaos::View{lyapExps, expsNum, 1};
+  a.accumulate = 1;
+  a.status = nullptr;
+  int rc = chaos::launch_compat(m->id, a, 64, (cudaStream_t)stream);
+  if (rc == chaos::kErrUnsupported) return fail(CHAOS_LYAP_EUNSUPPORTED, "no kernel for this k");
+  if (rc) return cuda_fail((cudaError_t)rc, "cudaLyapunov launch");
+  return CHAOS_LYAP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,68 @@
+// Launch-side declarations shared by the kernel translation units and the
+// C-ABI layer.  Plain structs of pointers and scalars; no torch types.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace chaos {
+
+// Strided view of a P x C array of doubles: element (point, comp) lives at
+// base[point * ps + comp * cs].  Point-major (the reference's layout,
+// tasklyapunov.cpp:47-71) is ps = C, cs = 1; component-major (SoA) is ps = 1,
+// cs = P.
+struct View {
+  double *base;
+  int64_t ps, cs;
+};
+struct CView {
+  const double *base;
+  int64_t ps, cs;
+};
+
+// Reference-exact fixed-step FP64 sweep: cuda/lyapunov.dp.cpp:5-259 (FD, VAR,
+// QR) with the DVERK step of cuda/tools/dverk.dp.cpp:7-81.
+struct CompatArgs {
+  int64_t P;
+  int32_t k, method;  // method: 0 FD, 1 VAR, 2 QR
+  double eps, step, t_skip, t_skip_clp, calc_time, add_skip;
+  CView params;
+  View inits;             // advanced in place to the end states
+  double *close;          // nullable: P*k*n, the final perturbation / tangent vectors
+  View lyap;              // P x k
+  int32_t accumulate;     // 1: start each sum from the value already in lyap
+  int32_t *status;        // nullable: 0 ok, 1 non-finite spectrum
+};
+
+// Adaptive forms (DVERK 6(5) or Dopri5; FP64 or FP32 state and tangent; FP64
+// Gram-Schmidt and compensated log-norm sums).
+struct AdaptiveArgs {
+  int64_t P;
+  int32_t k, gs;          // gs: 0 classical, 1 modified Gram-Schmidt
+  double rtol, atol, h0, hmax, hmin;
+  double t_transient, t_align, t_avg, dt_renorm;
+  int64_t max_steps;
+  double escape;          // a state component beyond this magnitude ends the point
+  CView params;
+  CView inits;
+  const double *t_avg_per_point;  // nullable: per-point averaging time
+  View spectrum;          // P x k
+  int32_t *status;        // nullable
+  int64_t *steps;         // nullable: attempted steps per point
+  // persistent work-queue form
+  unsigned long long *queue;  // nullable unless the launch is persistent
+};
+
+enum Integrator : int32_t { kDverkFixed = 0, kDverk65 = 1, kDopri5 = 2 };
+enum Precision : int32_t { kCompatFP64 = 0, kFP64 = 1, kFP32 = 2 };
+
+// Returns cudaSuccess or the launch error; kErrUnsupported for a combination
+// that has no instantiation.
+constexpr int kErrUnsupported = -1;
+
+int launch_compat(int model, const CompatArgs &a, int block, cudaStream_t s);
+int launch_adaptive(int model, int integrator, int precision, const AdaptiveArgs &a, int block,
+                    int persistent_blocks, cudaStream_t s);
+int launch_l96_warp(int integrator, int precision, const AdaptiveArgs &a, int warps_per_block,
+                    cudaStream_t s);
+
+}  // namespace chaos
