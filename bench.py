@@ -1,0 +1,380 @@
+"""Throughput of the Lyapunov-spectrum sweep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload rossler1024|lorenz64]
+
+Workload (default ``rossler1024``, the precision form): Rossler
+dx = -y - z, dy = x + a y, dz = b + z (x - c), b = 0.2, on a 1024 x 1024 grid
+a in [0.05, 0.45] x c in [2, 12]; x0 = (1, 1, 0) + U(-1e-3, 1e-3) seeded per
+point; Dormand-Prince 5(4) with state and tangent in FP32 (rtol = atol =
+1e-6), Gram-Schmidt and Kahan-compensated log-norm sums in FP64; transient
+500, averaging 5000 time units, renormalisation every 2.  One step = the
+whole map.  ``lorenz64``: Lorenz 64 x 64, sigma in [5, 20] x rho in [0, 200],
+beta = 8/3, DVERK 6(5) FP64 rtol = atol = 1e-10, transient 100, averaging
+1000, renormalisation every 1.
+
+Under torchrun each rank sweeps its own map (jitter seed = rank): weak
+scaling, no collective on the data path; the reported time is the maximum
+over ranks of the device-timed region.
+
+--impl reference times the reference's own implementation of this path (its
+sources compiled for the host: fixed-step DVERK, VAR method) on the host
+cores, on a bounded random sample of the same map.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "rossler1024": dict(
+        model="rossler", base=[0.2, 0.2, 5.7], s1=[0, 0.05, 0.45, 1024], s2=[2, 2.0, 12.0, 1024],
+        x0=[1.0, 1.0, 0.0], amp=1e-3, integrator="dopri5", precision="fp32", rtol=1e-6,
+        atol=1e-6, h=1e-2, t_transient=500.0, t_avg=5000.0, dt_renorm=2.0, dtype="fp32",
+        # reference arm: its fixed-step DVERK; 0.01 is the step its own config uses
+        ref_h=0.01),
+    "lorenz64": dict(
+        model="lorenz", base=[10.0, 28.0, 8.0 / 3.0], s1=[0, 5.0, 20.0, 64], s2=[1, 0.0, 200.0, 64],
+        x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dverk65", precision="fp64", rtol=1e-10,
+        atol=1e-10, h=1e-3, t_transient=100.0, t_avg=1000.0, dt_renorm=1.0, dtype="fp64",
+        ref_h=1e-3),
+}
+# Algorithmic flops per attempted step: S (F_f + k F_Jv) + 2 C n (1 + k),
+# S = new stages per step, C = tableau coefficients incl. output and error.
+STAGES = {"dopri5": (6, 26), "dverk65": (8, 39)}
+MODEL_FLOPS = {"rossler": (7, 8, 3), "lorenz": (9, 12, 3)}  # F_f, F_Jv, n
+
+
+def flops_per_step(model, integrator):
+    S, C = STAGES[integrator]
+    ff, fj, n = MODEL_FLOPS[model]
+    return S * (ff + n * fj) + 2 * C * n * (1 + n)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_inputs(w, seed):
+    import chaos_oneapi_b200 as cl
+    params = cl.make_grid(len(w["base"]), w["base"], w["s1"], w["s2"])
+    inits = cl.make_inits(len(w["x0"]), params.shape[0], w["x0"], w["amp"], "uniform", seed)
+    return params, inits
+
+
+def cpu_reference(w, params, inits, sample, threads, seed=0):
+    """The reference's implementation (oracle/_ref) on `sample` random points."""
+    import oracle
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(params.shape[0], sample, replace=False)
+    t0 = time.perf_counter()
+    out, _ = oracle.reference(w["model"], "var", params[idx], inits[idx], 1e-7, w["ref_h"], 3,
+                              w["t_transient"], 0.0, w["t_avg"], w["dt_renorm"] / w["ref_h"],
+                              threads=threads)
+    dt = time.perf_counter() - t0
+    return sample / dt, dt, idx, out
+
+
+def ref_seconds_per_point(w):
+    """Rough single-thread cost of one point in the reference (measured on a
+    2.7 GHz Xeon: 4.7 s for Rossler, T = 5500, h = 0.01), used only to size
+    the bounded CPU sample."""
+    return 4.7 * (w["t_transient"] + w["t_avg"]) / 5500.0 * (0.01 / w["ref_h"])
+
+
+def ref_kind():
+    import oracle
+    return "reference" if oracle.have_ref() else "port"
+
+
+def run_reference_arm(a, w, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    params, inits = build_inputs(w, 0)
+    # per step about 20 s of the host's threads
+    sample = int(max(threads, min(4096, 20.0 * threads / ref_seconds_per_point(w))))
+    for _ in range(a.warmup):
+        cpu_reference(w, params, inits, max(1, sample // 8), threads)
+    vals = []
+    t0 = time.perf_counter()
+    for s in range(a.steps):
+        v, _, _, _ = cpu_reference(w, params, inits, sample, threads, seed=s + 1)
+        vals.append(v)
+    total = time.perf_counter() - t0
+    value = sample * a.steps / total
+    kind = ref_kind()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * total / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+        "config": config_of(a, w, extra={"reference_integrator": f"fixed-step DVERK h={w['ref_h']}",
+                                          "sample_points_per_step": sample}),
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} random points of the map per step, "
+                                   f"fixed-step DVERK h={w['ref_h']}, VAR method"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "Lyapunov-spectrum points/s"
+
+
+def config_of(a, w, extra=None):
+    c = {"workload": a.workload, "model": w["model"],
+         "grid": f"{int(w['s1'][3])}x{int(w['s2'][3])}",
+         "integrator": w["integrator"], "precision": w["precision"], "rtol": w["rtol"],
+         "t_transient": w["t_transient"], "t_avg": w["t_avg"], "dt_renorm": w["dt_renorm"],
+         "global_points": int(w["s1"][3] * w["s2"][3]) * a.gpus,
+         "parallelism": f"points sharded: one map per rank x {a.gpus}",
+         "l2": "inputs 72 MB < L2; a 256 MB buffer is written between timed steps"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rossler1024", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-sample", type=int, default=256)
+    a = ap.parse_args()
+    w = WORKLOADS[a.workload]
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    a.gpus = max(a.gpus, world)
+
+    if a.impl == "reference":
+        run_reference_arm(a, w, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import chaos_oneapi_b200 as cl
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    params, inits = build_inputs(w, rank)
+    P = params.shape[0]
+    sw = cl.Sweep(model=w["model"], method="var", integrator=w["integrator"],
+                  precision=w["precision"], rtol=w["rtol"], atol=w["atol"], h=w["h"],
+                  t_transient=w["t_transient"], t_avg=w["t_avg"], dt_renorm=w["dt_renorm"],
+                  device=local, schedule="persistent")
+    dev = torch.device("cuda", local)
+    dp = torch.from_numpy(params).to(dev)
+    dx = torch.from_numpy(inits).to(dev)
+    ds = torch.empty((P, 3), dtype=torch.float64, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    steps = torch.empty(P, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(dev)
+
+    peak = cl.fma_peak_tflops(local, "fp32" if w["precision"] == "fp32" else "fp64", 1.0)
+
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            sw.run(dp, dx, ds, st, steps, stream=stream)
+        stream.synchronize()
+
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(a.steps)]
+        clocks = ClockSampler(local)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        clocks.start()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(a.steps):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            sw.run(dp, dx, ds, st, steps, stream=stream)
+            ev[i][1].record(stream)
+        t_end.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        clk = clocks.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    kernel_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / a.steps
+    if world > 1:
+        t = torch.tensor([elapsed_ms, kernel_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms, kernel_ms = t.tolist()
+
+    total_points = P * a.steps * world
+    value = total_points / (elapsed_ms * 1e-3)
+    steps_np = steps.cpu().numpy()
+    status_np = st.cpu().numpy()
+    spec_np = ds.cpu().numpy()
+    fl = float(steps_np.sum()) * flops_per_step(w["model"], w["integrator"])
+    achieved = fl / (kernel_ms * 1e-3) / 1e12
+
+    # end to end: host buffers (pinned) through the C ABI's host path
+    hp = torch.from_numpy(params).pin_memory()
+    hx = torch.from_numpy(inits).pin_memory()
+    hs = torch.empty((P, 3), dtype=torch.float64).pin_memory()
+    hst = torch.empty(P, dtype=torch.int32).pin_memory()
+    e2e_steps = 1
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        cl.native.check(cl.native.lib.chaos_lyap_run_host(
+            sw._h, P, cl.sweep.ctypes.c_void_p(hp.data_ptr()),
+            cl.sweep.ctypes.c_void_p(hx.data_ptr()), cl.sweep.ctypes.c_void_p(hs.data_ptr()),
+            cl.sweep.ctypes.c_void_p(hst.data_ptr()), None, None))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e = {"value": P * e2e_steps * world / e2e_s, "unit": "points/s",
+           "h2d_bytes_per_step": int(hp.numel() * 8 + hx.numel() * 8),
+           "d2h_bytes_per_step": int(hs.numel() * 8 + hst.numel() * 4), "steps": e2e_steps}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", f"traffic_{a.workload}.txt")
+    if os.path.exists(tpath):  # DRAM bytes per launch from the committed ncu capture
+        for ln in open(tpath):
+            if ln.startswith("dram_bytes_per_launch_full"):
+                traffic = float(ln.split("=")[1])
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": w["dtype"], "data": "synthetic (seeded grid and jitter)",
+        "config": config_of(a, w),
+        "gpu_launches": a.steps,
+        "clocks": clk,
+        "roofline": {"bound": "fp32_fma" if w["precision"] == "fp32" else "fp64_fma",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": "measured in-process (FMA-chain kernel, chaos_lyap_fma_peak)",
+                     "flops_per_step": flops_per_step(w["model"], w["integrator"]),
+                     "kernel_ms": kernel_ms},
+        "e2e": e2e,
+        "points": {"ok": int((status_np == 0).sum()), "escaped": int((status_np == 4).sum()),
+                   "other": int(((status_np != 0) & (status_np != 4)).sum()),
+                   "steps_mean": float(steps_np.mean()), "steps_max": int(steps_np.max())},
+    }
+
+    # accuracy against the FP64 oracle (rtol 1e-12) on a random sample
+    if a.accuracy_sample > 0:
+        import oracle
+        rng = np.random.default_rng(1234)
+        idx = rng.choice(P, a.accuracy_sample, replace=False)
+        ref, rst, _ = oracle.adaptive(w["model"], params[idx], inits[idx], 3,
+                                      integrator="dverk65", rtol=1e-12, atol=1e-12,
+                                      t_transient=w["t_transient"], t_avg=w["t_avg"],
+                                      dt_renorm=w["dt_renorm"])
+        ok = (rst == 0) & (status_np[idx] == 0)
+        d = np.abs(spec_np[idx][ok] - ref[ok])
+        chaotic = ref[ok][:, 0] > 0.01
+        line["accuracy"] = {
+            "vs": "FP64 adaptive oracle, DVERK 6(5) rtol=atol=1e-12 (CPU)",
+            "sample": int(a.accuracy_sample), "compared": int(ok.sum()),
+            "status_agree": float((rst == status_np[idx]).mean()),
+            "frac_all_within_1e-3": float((d.max(axis=1) <= 1e-3).mean()),
+            "frac_within_1e-3_per_exponent": [float(x) for x in (d <= 1e-3).mean(axis=0)],
+            "median_abs_err": [float(x) for x in np.median(d, axis=0)],
+            "max_abs_err_regular": [float(x) for x in d[~chaotic].max(axis=0)] if (~chaotic).any() else None,
+            "chaotic_cells": int(chaotic.sum()),
+            "regime_sign_agreement": float((np.sign(spec_np[idx][ok][:, 0] - 0.01) ==
+                                            np.sign(ref[ok][:, 0] - 0.01)).mean()),
+        }
+
+    if not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = int(max(threads, min(2048, 15.0 * threads / ref_seconds_per_point(w))))
+        v, dt, _, _ = cpu_reference(w, params, inits, sample, threads)
+        line["cpu_baseline"] = {"value": v, "unit": "points/s", "cores": threads,
+                                "kind": ref_kind(),
+                                "sample": f"{sample} random points of the same map, fixed-step "
+                                          f"DVERK h={w['ref_h']} (VAR method), {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

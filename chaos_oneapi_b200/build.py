@@ -37,6 +37,7 @@ CUDA_UNITS = {
     "adaptive.cu": [],
     "l96.cu": [],
     "capi.cu": [],
+    "peak.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]
 HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp"]

@@ -13,14 +13,23 @@
 namespace chaos {
 namespace adaptive {
 
+// The queue hands out points in the order q -> (q * stride) mod P (stride
+// coprime to P, so a permutation): neighbouring grid points cost alike, and
+// spreading them over the run keeps a cluster of expensive points (a chaotic
+// band, escaping orbits) from forming the tail of the launch.
+__device__ __forceinline__ int64_t next_point(const AdaptiveArgs &a) {
+  const unsigned long long q = atomicAdd(a.queue, 1ULL);
+  if (q >= (unsigned long long)a.P) return a.P;
+  return (int64_t)((q * (unsigned long long)a.queue_stride) % (unsigned long long)a.P);
+}
+
 template <class M, int K, class R, int INTEG>
 __global__ void __launch_bounds__(128) sweep_kernel(const AdaptiveArgs a) {
-  int64_t pt = a.queue ? (int64_t)atomicAdd(a.queue, 1ULL)
-                       : (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t pt = a.queue ? next_point(a) : (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   while (pt < a.P) {
     run_point<M, K, R, INTEG>(a, pt);
     if (!a.queue) break;
-    pt = (int64_t)atomicAdd(a.queue, 1ULL);
+    pt = next_point(a);
   }
 }
 

@@ -15,9 +15,11 @@
 //    arithmetic as one RK step of the joint (n + k n)-dimensional system, with
 //    a register footprint of one vector's stages instead of all of them.
 //  * Renormalisation at every multiple of dt_renorm (steps are clamped to
-//    land on it): Gram-Schmidt (classical as cuda/tools/linalg.dp.cpp:36-51,
-//    or modified) in FP64 whatever the state precision, log-norms summed in
-//    FP64 with Kahan compensation.
+//    land on it), each interval split per point into as many equal parts as
+//    the spread of the tangent directions needs (see run_point): Gram-Schmidt
+//    (classical as cuda/tools/linalg.dp.cpp:36-51, or modified) in FP64
+//    whatever the state precision, log-norms summed in FP64 with Kahan
+//    compensation.
 #pragma once
 #include "kernels.h"
 #include "models.cuh"
@@ -381,6 +383,15 @@ CL_HD void renormalise(R (&V)[K][N], double (&r)[K], int gs) {
     for (int j = 0; j < N; j++) V[i][j] = (R)v[i][j];
 }
 
+constexpr int kRenormSubInit = 16, kRenormSubMax = 64;
+
+// Largest log-norm spread allowed within one renormalisation sub-interval:
+// 0.3 ln(1 / max(rtol, unit roundoff of R)).
+template <class R> CL_HD float renorm_spread_limit(float rtol) {
+  const float ulp = sizeof(R) == 4 ? 5.96e-8f : 1.2e-16f;
+  return 0.3f * logf(1.0f / fmaxf(rtol, ulp));
+}
+
 // Whole per-point computation.  Returns the status code.
 template <class M, int K, class R, int INTEG>
 CL_HD int run_point(const AdaptiveArgs &a, int64_t pt) {
@@ -396,7 +407,7 @@ CL_HD int run_point(const AdaptiveArgs &a, int64_t pt) {
   // A step below 1e-12 (model time units) is never meaningful here; it also
   // stops a point whose controller collapsed the step to zero.
   const Ctl c{(float)a.rtol, (float)a.atol, a.hmax > 0 ? a.hmax : 1e300, fmax(a.hmin, 1e-12),
-              a.max_steps, a.escape > 0 ? a.escape : 1e300};
+              a.max_steps, a.escape > 0 ? a.escape : 1e4};
   const double t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
 
   int status = 0;
@@ -412,31 +423,56 @@ CL_HD int run_point(const AdaptiveArgs &a, int64_t pt) {
   for (int i = 0; i < K; i++) sum[i] = comp[i] = 0.0;
   const double total = a.t_align + t_avg;
   const double eps_t = 1e-12 * total;
+  // Renormalisation sub-intervals.  The exponent estimate is the same for any
+  // renormalisation schedule (the R factors of successive Gram-Schmidt steps
+  // multiply to the R factor of the whole interval), but the weakest tangent
+  // direction is only resolved while its share of each tangent vector stays
+  // above the integration error.  So each dt_renorm interval is split into m
+  // equal parts, and m adapts per point to the spread of log-norms seen in one
+  // part: doubled when it exceeds tau, halved when below tau / 4.
+  const float tau = renorm_spread_limit<R>(c.rtol);
+  int m = kRenormSubInit;
   double t = 0.0;
   while (status == 0 && t < total) {
     double len = a.dt_renorm;
     if (t + len > total) len = total - t;
-    status = integrate<M, K, R, INTEG, true>(st, len, c);
-    if (status) break;
-    t += len;
-    double r[K];
-    renormalise<N, K, R>(st.V, r, a.gs);
-    bool ok = true;
+    const double sub = len / m;
+    float max_spread = 0.f;
+    for (int j = 0; j < m; j++) {
+      const double l = (j == m - 1) ? len - sub * (m - 1) : sub;
+      status = integrate<M, K, R, INTEG, true>(st, l, c);
+      if (status) break;
+      double r[K];
+      renormalise<N, K, R>(st.V, r, a.gs);
+      bool ok = true;
 #pragma unroll
-    for (int i = 0; i < K; i++) ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
-    if (!ok) {
-      status = 1;
-      break;
-    }
-    if (t > a.t_align + eps_t) {
+      for (int i = 0; i < K; i++) ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
+      if (!ok) {
+        status = 1;
+        break;
+      }
+      double lg[K];
+      double lmax = -1e300, lmin = 1e300;
 #pragma unroll
-      for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
-        const double y = log(r[i]) - comp[i];
-        const double s = sum[i] + y;
-        comp[i] = (s - sum[i]) - y;
-        sum[i] = s;
+      for (int i = 0; i < K; i++) {
+        lg[i] = log(r[i]);
+        lmax = fmax(lmax, lg[i]);
+        lmin = fmin(lmin, lg[i]);
+      }
+      max_spread = fmaxf(max_spread, (float)(lmax - lmin));
+      if (t + sub * (j + 1) > a.t_align + eps_t) {
+#pragma unroll
+        for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
+          const double y = lg[i] - comp[i];
+          const double s2 = sum[i] + y;
+          comp[i] = (s2 - sum[i]) - y;
+          sum[i] = s2;
+        }
       }
     }
+    t += len;
+    if (max_spread > tau && m < kRenormSubMax) m *= 2;
+    else if (max_spread < 0.25f * tau && m > 1) m /= 2;
   }
 #pragma unroll
   for (int i = 0; i < K; i++) {

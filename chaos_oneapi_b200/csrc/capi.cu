@@ -125,7 +125,7 @@ int chaos_lyap_desc_init(chaos_lyap_desc *d) {
   d->h = 1e-3;
   d->rtol = d->atol = 1e-10;
   d->max_steps = 100000000LL;
-  d->escape = 1e8;
+  d->escape = 1e4;
   d->schedule = CHAOS_SCHED_AUTO;
   return CHAOS_LYAP_OK;
 }
@@ -304,7 +304,7 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
     a.t_avg = t_avg_override > 0 ? t_avg_override : d.t_avg;
     a.dt_renorm = d.dt_renorm;
     a.max_steps = d.max_steps;
-    a.escape = d.escape > 0 ? d.escape : 1e8;
+    a.escape = d.escape > 0 ? d.escape : 1e4;
     a.params = cview(params, P, m->nparams, d.layout);
     a.inits = cview(inits, P, m->dim, d.layout);
     a.t_avg_per_point = t_avg_override > 0 ? nullptr : tavg;
@@ -319,6 +319,7 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
       cudaError_t e = cudaMemsetAsync(h->queue, 0, sizeof(unsigned long long), s);
       if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
       a.queue = h->queue;
+      a.queue_stride = chaos::queue_stride_for(P);
       rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);
     } else {
       rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);

@@ -50,7 +50,18 @@ struct AdaptiveArgs {
   int64_t *steps;         // nullable: attempted steps per point
   // persistent work-queue form
   unsigned long long *queue;  // nullable unless the launch is persistent
+  uint64_t queue_stride;      // coprime to P: hand-out order q -> q * stride mod P
 };
+
+// A stride for the persistent queue's permutation: a prime that does not
+// divide P (so q -> q * stride mod P is a bijection on [0, P)).
+inline uint64_t queue_stride_for(int64_t P) {
+  if (P <= 1) return 1;
+  const uint64_t primes[] = {1000003ULL, 1000033ULL, 1000037ULL, 1000039ULL};
+  for (uint64_t s : primes)
+    if ((uint64_t)P % s != 0) return s;  // s prime and s does not divide P: gcd = 1
+  return 1;
+}
 
 enum Integrator : int32_t { kDverkFixed = 0, kDverk65 = 1, kDopri5 = 2 };
 enum Precision : int32_t { kCompatFP64 = 0, kFP64 = 1, kFP32 = 2 };

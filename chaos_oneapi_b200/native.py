@@ -86,6 +86,8 @@ SIGNATURES = {
         _P, _P, ctypes.c_int32, ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_double,
         ctypes.c_double, _P, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
         ctypes.c_double, _P]),
+    "chaos_lyap_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_double)]),
     "chaos_lyap_make_grid": (ctypes.c_int64, [ctypes.c_int32, _D, _D, _D, _D]),
     "chaos_lyap_make_inits": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, _D, ctypes.c_double,
                                              ctypes.c_int32, ctypes.c_uint64, _D]),

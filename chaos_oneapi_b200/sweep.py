@@ -83,7 +83,7 @@ class SweepConfig:
     t_avg: float = 1.0
     dt_renorm: float = 1.0
     max_steps: int = 100_000_000
-    escape: float = 1e8
+    escape: float = 1e4
     device: int = 0
     schedule: str = "auto"       # auto | direct | persistent
     block: int = 0
@@ -220,3 +220,11 @@ def cuda_lyapunov(task_num, is_qr, is_var, inits, close_points, dimension, model
         model.encode(), _tptr(params, "float64"), params_dim, eps, step,
         _tptr(lyap_exps, "float64"), exps_num, time_skip, time_skip_clp, calc_time,
         add_skip_steps, ctypes.c_void_p(stream)))
+
+
+def fma_peak_tflops(device: int = 0, precision: str = "fp32", seconds: float = 0.5) -> float:
+    """Measured FMA-pipe throughput (TFLOP/s) of `device`: the roofline
+    denominator of the sweep kernels."""
+    out = ctypes.c_double()
+    check(lib.chaos_lyap_fma_peak(device, native.PREC[precision], seconds, ctypes.byref(out)))
+    return out.value

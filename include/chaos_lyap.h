@@ -98,7 +98,7 @@ typedef struct chaos_lyap_desc {
   int32_t schedule;         /* CHAOS_SCHED_* */
   int32_t block;            /* threads per block, 0 = tuned default */
   int32_t reserved0;
-  double escape;            /* adaptive: escape radius of the state (0: 1e8) */
+  double escape;            /* adaptive: escape radius of the state (0: 1e4) */
   int32_t reserved[4];
 } chaos_lyap_desc;
 
@@ -112,7 +112,7 @@ const char *chaos_lyap_last_error(void);
 
 /* Fills desc with defaults: VAR, DVERK 6(5), FP64, classical GS, k = 0
  * (= model dimension at create), point-major, eps 1e-7, h 1e-3, rtol = atol
- * = 1e-10, max_steps 1e8, escape radius 1e8. */
+ * = 1e-10, max_steps 1e8, escape radius 1e4. */
 int chaos_lyap_desc_init(chaos_lyap_desc *desc);
 
 /* Model registry (replaces the registry lookups of tasklyapunov.cpp:15-16 and
@@ -195,6 +195,13 @@ int64_t chaos_lyap_make_grid(int32_t nparams, const double *base_params, const d
  * regenerated independently. */
 int chaos_lyap_make_inits(int32_t dim, int64_t P, const double *base, double amp, int32_t dist,
                           uint64_t seed, double *out);
+
+/* Measures the FP32 (precision = CHAOS_PREC_FP32) or FP64 (CHAOS_PREC_FP64)
+ * fused-multiply-add throughput of `device` with a kernel of independent FMA
+ * chains running for about `seconds`; the roofline denominator of the sweep
+ * kernels, which are bound by the FMA pipe.  No reference counterpart (the
+ * reference reports whole-run wall time only, raiitimer.h). */
+int chaos_lyap_fma_peak(int device, int precision, double seconds, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -126,7 +126,7 @@ def reference(model: str, method: str, params, inits, eps, h, k, t_skip, t_skip_
 
 def adaptive(model: str, params, inits, k, integrator="dverk65", gs="cgs", rtol=1e-12,
              atol=1e-12, h0=1e-3, hmax=0.0, hmin=0.0, t_transient=0.0, t_align=0.0, t_avg=1.0,
-             dt_renorm=1.0, max_steps=10**8, escape=1e8, threads: int = 0):
+             dt_renorm=1.0, max_steps=10**8, escape=1e4, threads: int = 0):
     """FP64 adaptive oracle.  Returns (spectrum, status, steps)."""
     params, x = _c(params), _c(inits)
     P = params.shape[0]

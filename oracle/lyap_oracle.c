@@ -593,39 +593,60 @@ static void adaptive_point(void *a, int64_t i) {
   s.N = Nj;
   s.fac_old = 1e-4;
   const double total = cfg->t_align + cfg->t_avg;
+  /* Renormalisation sub-intervals, the same per-point policy as the device
+   * kernels: each dt_renorm interval is split into m equal parts, m doubled
+   * when one part's log-norm spread exceeds tau = 0.3 ln(1/max(rtol, u)),
+   * halved when below tau / 4 (m in 1..64, starting at 16). */
+  const float tau = 0.3f * logf(1.0f / fmaxf((float)cfg->rtol, 1.2e-16f));
+  int m = 16;
   double t = 0;
   while (!st && t < total) {
     double len = cfg->dt_renorm;
     if (t + len > total) len = total - t;
-    s.have_k1 = 0;
-    st = integrate(&s, y, len);
-    if (st) break;
-    t += len;
-    /* Gram-Schmidt on the tangent vectors (CGS as linalg.dp.cpp:36-51, or MGS) */
-    double *V = y + n;
-    for (int q = 0; q < k; q++) {
-      double *vq = V + q * n;
-      if (cfg->gs == ORC_MGS) {
-        for (int pq = 0; pq < q; pq++) {
-          double c = dot_seq(V + pq * n, vq, n);
-          for (int c2 = 0; c2 < n; c2++) vq[c2] -= c * V[pq * n + c2];
+    const double sub = len / m;
+    float max_spread = 0.f;
+    for (int jj = 0; jj < m; jj++) {
+      const double l = (jj == m - 1) ? len - sub * (m - 1) : sub;
+      s.have_k1 = 0;
+      st = integrate(&s, y, l);
+      if (st) break;
+      /* Gram-Schmidt on the tangent vectors (CGS as linalg.dp.cpp:36-51, or MGS) */
+      double *V = y + n;
+      for (int q = 0; q < k; q++) {
+        double *vq = V + q * n;
+        if (cfg->gs == ORC_MGS) {
+          for (int pq = 0; pq < q; pq++) {
+            double c = dot_seq(V + pq * n, vq, n);
+            for (int c2 = 0; c2 < n; c2++) vq[c2] -= c * V[pq * n + c2];
+          }
+        } else {
+          double proj[L96_N];
+          for (int c2 = 0; c2 < n; c2++) proj[c2] = 0;
+          for (int pq = 0; pq < q; pq++) {
+            double c = dot_seq(V + pq * n, vq, n);
+            for (int c2 = 0; c2 < n; c2++) proj[c2] += c * V[pq * n + c2];
+          }
+          for (int c2 = 0; c2 < n; c2++) vq[c2] -= proj[c2];
         }
-      } else {
-        double proj[L96_N];
-        for (int c2 = 0; c2 < n; c2++) proj[c2] = 0;
-        for (int pq = 0; pq < q; pq++) {
-          double c = dot_seq(V + pq * n, vq, n);
-          for (int c2 = 0; c2 < n; c2++) proj[c2] += c * V[pq * n + c2];
-        }
-        for (int c2 = 0; c2 < n; c2++) vq[c2] -= proj[c2];
+        r[q] = norm_seq(vq, n);
+        for (int c2 = 0; c2 < n; c2++) vq[c2] /= r[q];
       }
-      r[q] = norm_seq(vq, n);
-      for (int c2 = 0; c2 < n; c2++) vq[c2] /= r[q];
+      for (int q = 0; q < k; q++)
+        if (!isfinite(r[q]) || r[q] <= 0) st = 1;
+      if (st) break;
+      double lmax = -1e300, lmin = 1e300;
+      for (int q = 0; q < k; q++) {
+        double lg = log(r[q]);
+        lmax = fmax(lmax, lg);
+        lmin = fmin(lmin, lg);
+      }
+      if ((float)(lmax - lmin) > max_spread) max_spread = (float)(lmax - lmin);
+      if (t + sub * (jj + 1) > cfg->t_align + 1e-12 * total)
+        for (int q = 0; q < k; q++) sums[q] += logl((long double)r[q]);
     }
-    if (t > cfg->t_align + 1e-12 * total)
-      for (int q = 0; q < k; q++) sums[q] += logl((long double)r[q]);
-    for (int q = 0; q < k; q++)
-      if (!isfinite(r[q]) || r[q] <= 0) st = 1;
+    t += len;
+    if (max_spread > tau && m < 64) m *= 2;
+    else if (max_spread < 0.25f * tau && m > 1) m /= 2;
   }
   for (int q = 0; q < k; q++) o[q] = st ? NAN : (double)(sums[q] / (long double)cfg->t_avg);
   if (j->status) j->status[i] = st;
