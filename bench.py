@@ -44,6 +44,12 @@ WORKLOADS = {
         atol=1e-6, h=1e-2, t_transient=500.0, t_avg=5000.0, dt_renorm=2.0, dtype="fp32",
         # reference arm: its fixed-step DVERK; 0.01 is the step its own config uses
         ref_h=0.01),
+    # a small case of the same kernel, for profiler captures
+    "rossler_small": dict(
+        model="rossler", base=[0.2, 0.2, 5.7], s1=[0, 0.05, 0.45, 256], s2=[2, 2.0, 12.0, 256],
+        x0=[1.0, 1.0, 0.0], amp=1e-3, integrator="dopri5", precision="fp32", rtol=1e-6,
+        atol=1e-6, h=1e-2, t_transient=50.0, t_avg=500.0, dt_renorm=2.0, dtype="fp32",
+        ref_h=0.01),
     "lorenz64": dict(
         model="lorenz", base=[10.0, 28.0, 8.0 / 3.0], s1=[0, 5.0, 20.0, 64], s2=[1, 0.0, 200.0, 64],
         x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dverk65", precision="fp64", rtol=1e-10,

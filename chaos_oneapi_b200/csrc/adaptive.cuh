@@ -77,11 +77,19 @@ CL_HD double quiet_nan() {
 #endif
 }
 
-// Error weight contribution of one component.
+// Error weight contribution of one component (the error norm only steers the
+// step length, so an approximate reciprocal is enough).
+CL_HD float fast_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
 template <class R>
 CL_HD float err_term(R y0, R y1, R e, float rtol, float atol) {
   const float m = fmaxf(fabsf((float)y0), fabsf((float)y1));
-  const float r = (float)e / (atol + rtol * m);
+  const float r = fast_div((float)e, fmaf(rtol, m, atol));
   return r * r;
 }
 
@@ -262,7 +270,7 @@ CL_HD float attempt(PointState<M, K, R, INTEG> &st, R h, float rtol, float atol,
     }
   }
   constexpr int NC = JOINT ? N * (1 + K) : N;
-  return sqrtf(err2 * (1.0f / NC));
+  return sqrtf(err2 * (1.0f / NC));  // err2 >= 0
 }
 
 struct Ctl {
@@ -301,8 +309,8 @@ CL_HD int integrate(PointState<M, K, R, INTEG> &st, double len, const Ctl &c) {
     if (!(err == err) || err > 3.0e38f) return 1;
     const float fac11 = exp2f(expo1 * fast_log2f(fmaxf(err, 1e-30f)));
     float fac = fac11 * exp2f(-beta * fast_log2f(st.fac_old));
-    fac = fmaxf(facc2, fminf(facc1, fac / safe));
-    R hnew = h / (R)fac;
+    fac = fmaxf(facc2, fminf(facc1, fac * (1.0f / safe)));
+    R hnew = h * (R)fast_div(1.0f, fac);
     if (err <= 1.0f) {
       st.fac_old = fmaxf(err, 1e-4f);
 #pragma unroll
@@ -326,10 +334,10 @@ CL_HD int integrate(PointState<M, K, R, INTEG> &st, double len, const Ctl &c) {
       if (!clamped || hnew < h) st.h = hnew;
       bool inside = true;
 #pragma unroll
-      for (int j = 0; j < N; j++) inside = inside && (fabs((double)st.x[j]) <= c.escape);
+      for (int j = 0; j < N; j++) inside = inside && (fabs(st.x[j]) <= (R)c.escape);
       if (!inside) return 4;
     } else {
-      st.h = h / (R)fminf(facc1, fac11 / safe);
+      st.h = h * (R)fast_div(1.0f, fminf(facc1, fac11 * (1.0f / safe)));
       reject = true;
     }
   }

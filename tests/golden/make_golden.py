@@ -1,0 +1,59 @@
+"""Generates tests/golden/reference_fixed.npz from the reference's own
+sources built for the host (oracle/_ref/libchaos_ref.so; recipe in
+oracle/Makefile).  Run here, where the reference tree is available:
+
+    python tests/golden/make_golden.py
+
+Each case is one model x method on a few seeded points with short phase
+times; the fixture stores the inputs, the spectra and the end states the
+reference produced.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+import oracle  # noqa: E402
+
+# model: (param base, init base, k, h, t_skip, t_clp, t_calc, dt_norm)
+CASES = {
+    "shimizu": ([0.8, 0.5], [0.1, 0.0, 0.0], 3, 0.01, 5.0, 2.0, 10.0, 0.5),
+    "lorenz": ([10.0, 28.0, 8.0 / 3.0], [1.0, 1.0, 1.0], 3, 0.01, 5.0, 1.0, 10.0, 0.5),
+    "rossler": ([0.2, 0.2, 5.7], [1.0, 1.0, 0.0], 3, 0.01, 5.0, 1.0, 10.0, 0.5),
+    "chua": ([9.0, 14.3, -8.0 / 7.0, -5.0 / 7.0], [0.1, 0.0, 0.0], 3, 0.01, 5.0, 1.0, 10.0, 0.5),
+    "hyper_rossler": ([0.5, 0.05], [-10.0, -6.0, 0.0, 10.0], 4, 0.005, 2.0, 1.0, 5.0, 0.25),
+    "lorenz96": ([8.0, 1.0], [8.0] * 40, 40, 0.01, 0.5, 0.1, 0.5, 0.1),
+}
+P = 5
+
+
+def case_inputs(model, seed=7):
+    pb, xb = CASES[model][0], CASES[model][1]
+    rng = np.random.default_rng(seed)
+    params = np.array(pb)[None, :] * (1 + 0.02 * rng.uniform(-1, 1, (P, len(pb))))
+    inits = oracle.make_inits(len(xb), P, xb, 1e-2 if model == "lorenz96" else 1e-3, 0, seed)
+    return params, inits
+
+
+def main():
+    out = {}
+    for model, (pb, xb, k, h, ts, tc, tt, dn) in CASES.items():
+        params, inits = case_inputs(model)
+        for method in ("fd", "var", "qr"):
+            kk = k if (method == "qr" or model != "lorenz96") else 5
+            spec, x_end = oracle.reference(model, method, params, inits, 1e-7, h, kk, ts, tc, tt,
+                                           dn / h, threads=4)
+            key = f"{model}_{method}"
+            out[key + "_params"] = params
+            out[key + "_inits"] = inits
+            out[key + "_spec"] = spec
+            out[key + "_end"] = x_end
+            out[key + "_cfg"] = np.array([kk, h, ts, tc, tt, dn / h, 1e-7])
+    np.savez_compressed(os.path.join(HERE, "reference_fixed.npz"), **out)
+    print("wrote", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()
