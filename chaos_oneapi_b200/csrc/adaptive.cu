@@ -23,13 +23,34 @@ __device__ __forceinline__ int64_t next_point(const AdaptiveArgs &a) {
   return (int64_t)((q * (unsigned long long)a.queue_stride) % (unsigned long long)a.P);
 }
 
+// Each lane owns one point at a time and runs it as a state machine (one
+// step attempt per loop iteration), so a lane never waits for another lane's
+// phase or renormalisation interval to end: when its point is done it takes
+// the next one from the queue (persistent form) and carries on.  Gram-Schmidt
+// is voted per warp: when any lane is due, every lane past its transient
+// renormalises in the same pass.
 template <class M, int K, class R, int INTEG>
 __global__ void __launch_bounds__(128) sweep_kernel(const AdaptiveArgs a) {
+  const Ctl c = make_ctl<R>(a);
+  Lane<M, K, R, INTEG> L;
   int64_t pt = a.queue ? next_point(a) : (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  while (pt < a.P) {
-    run_point<M, K, R, INTEG>(a, pt);
-    if (!a.queue) break;
-    pt = next_point(a);
+  bool active = pt < a.P;
+  if (active) lane_start(L, a, pt);
+  while (__any_sync(0xffffffffu, active)) {
+    if (active && lane_step(L, a, c) == kFinished) {
+      pt = a.queue ? next_point(a) : a.P;
+      active = pt < a.P;
+      if (active) lane_start(L, a, pt);
+    }
+    const bool due = active && L.phase != kTransient && L.t_gs >= L.L;
+    if (__any_sync(0xffffffffu, due)) {
+      if (active && L.phase != kTransient && L.t_gs > 0.0 && !lane_gram_schmidt(L, a, c)) {
+        lane_finish(L, a, 1);
+        pt = a.queue ? next_point(a) : a.P;
+        active = pt < a.P;
+        if (active) lane_start(L, a, pt);
+      }
+    }
   }
 }
 

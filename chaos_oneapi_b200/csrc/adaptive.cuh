@@ -14,12 +14,10 @@
 //    each tangent vector runs the same stages with J(X_s).  This is the same
 //    arithmetic as one RK step of the joint (n + k n)-dimensional system, with
 //    a register footprint of one vector's stages instead of all of them.
-//  * Renormalisation at every multiple of dt_renorm (steps are clamped to
-//    land on it), each interval split per point into as many equal parts as
-//    the spread of the tangent directions needs (see run_point): Gram-Schmidt
-//    (classical as cuda/tools/linalg.dp.cpp:36-51, or modified) in FP64
-//    whatever the state precision, log-norms summed in FP64 with Kahan
-//    compensation.
+//  * Renormalisation (see Lane): Gram-Schmidt (classical as
+//    cuda/tools/linalg.dp.cpp:36-51, or modified) in FP64 whatever the state
+//    precision, at intervals of at most dt_renorm and exactly at the phase
+//    ends; log-norms summed in FP64 with Kahan compensation.
 #pragma once
 #include "kernels.h"
 #include "models.cuh"
@@ -201,24 +199,9 @@ CL_HD void dopri_pass(const R *y, const R *k1, R h, const F &fn, R *y1, R *k7,
   }
 }
 
-// Per-point integrator state.
-template <class M, int K, class R, int INTEG>
-struct PointState {
-  static constexpr int N = M::N;
-  static constexpr int S = (INTEG == kDverk65) ? 8 : 7;
-  R p[M::NP];
-  R x[N];
-  R V[K][N];
-  R kx[N];      // Dopri5 FSAL: derivative of the state
-  R kv[K][N];   // Dopri5 FSAL: derivatives of the tangent vectors
-  R h;
-  float fac_old;
-  int64_t steps;
-};
-
 // Stage evaluators for the state pass (records stage points) and the tangent
 // passes (J at the recorded stage points).
-template <class M, class R, int S>
+template <class M, class R>
 struct StateStages {
   const R *p;
   R (*X)[M::N];  // X[s] for s >= 1; stage 0 is the current state
@@ -230,7 +213,7 @@ struct StateStages {
     M::f(arg, out, p);
   }
 };
-template <class M, class R, int S>
+template <class M, class R>
 struct TangentStages {
   const R *p;
   const R *x0;
@@ -240,108 +223,81 @@ struct TangentStages {
   }
 };
 
-// Attempt one step of length h.  JOINT: also advance the tangent vectors.
-// On return x1/V1 (and, for Dopri5, kx1/kv1) hold the candidate; err is the
-// RMS weighted error over all integrated components.
-template <class M, int K, class R, int INTEG, bool JOINT>
-CL_HD float attempt(PointState<M, K, R, INTEG> &st, R h, float rtol, float atol,
-                                         R (&x1)[M::N], R (&V1)[K][M::N], R (&kx1)[M::N],
-                                         R (&kv1)[K][M::N]) {
+enum Phase : int32_t { kTransient = 0, kAlign = 1, kAverage = 2 };
+enum LaneResult : int32_t { kRunning = 0, kFinished = 1 };
+
+constexpr int kRenormSplitInit = 16, kRenormSplitMax = 64;
+
+// Largest log-norm spread allowed between two Gram-Schmidt steps:
+// 0.3 ln(1 / max(rtol, unit roundoff of R)).
+template <class R> CL_HD float renorm_spread_limit(float rtol) {
+  const float ulp = sizeof(R) == 4 ? 5.96e-8f : 1.2e-16f;
+  return 0.3f * logf(1.0f / fmaxf(rtol, ulp));
+}
+
+struct Ctl {
+  float rtol, atol, tau;
+  double hmax, hmin;
+  int64_t max_steps;
+  double escape;
+};
+
+// The whole integration state of one parameter point, owned by one lane.
+//
+// Phases: transient (state only) over t_transient; alignment (state +
+// tangent, renormalised, not accumulated) over t_align; averaging over t_avg.
+// Steps are clamped to land exactly on each phase end.  Between phase ends,
+// Gram-Schmidt runs whenever the time since the last one reaches the point's
+// interval L (<= dt_renorm), and -- in the device kernel -- whenever any lane
+// of the warp runs it, so that the whole warp renormalises in one pass
+// instead of one lane at a time.  The exponent estimate does not depend on
+// when renormalisations happen (the R factors of successive Gram-Schmidt steps
+// multiply to the R factor over the whole window); L only keeps the weakest
+// tangent direction above the integration error: it adapts so that the
+// spread of log-norms over one interval, at the largest recent spread rate,
+// stays near tau / 2.
+template <class M, int K, class R, int INTEG>
+struct Lane {
+  static constexpr int N = M::N;
+  R p[M::NP];
+  R x[N];
+  R V[K][N];
+  R kx[N];      // Dopri5 FSAL: derivative of the state
+  R kv[K][N];   // Dopri5 FSAL: derivatives of the tangent vectors
+  R h;
+  float fac_old;
+  int32_t phase;
+  bool reject;
+  double t_phase, phase_len;  // time into the current phase, its length
+  double t_gs, L;             // time since the last Gram-Schmidt, its target
+  double rate_max;            // largest recent log-norm spread per unit time
+  double t_avg;
+  double sum[K], comp[K];     // Kahan-compensated sums of log-norms
+  int64_t steps;
+  int64_t pt;
+};
+
+// Attempt one step of length h; the tangent vectors only when `joint`.
+template <class M, int K, class R, int INTEG>
+CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol, float atol,
+                    R (&x1)[M::N], R (&V1)[K][M::N], R (&kx1)[M::N], R (&kv1)[K][M::N]) {
   constexpr int N = M::N;
-  constexpr int S = PointState<M, K, R, INTEG>::S;
+  constexpr int S = (INTEG == kDverk65) ? 8 : 7;
   R X[S][N];
   float err2 = 0.f;
-  StateStages<M, R, S> fs{st.p, X};
-  if (INTEG == kDverk65) {
-    dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
-  } else {
-    dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
-  }
-  if (JOINT) {
-    if (INTEG == kDopri5) {
-#pragma unroll
-      for (int j = 0; j < N; j++) X[6][j] = x1[j];
-    }
-    TangentStages<M, R, S> ft{st.p, st.x, X};
+  StateStages<M, R> fs{st.p, X};
+  if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
+  else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
+  if (joint) {
+    TangentStages<M, R> ft{st.p, st.x, X};
 #pragma unroll
     for (int i = 0; i < K; i++) {
       if (INTEG == kDverk65) dverk_pass<N, R>(st.V[i], h, ft, V1[i], err2, rtol, atol);
       else dopri_pass<N, R>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
     }
   }
-  constexpr int NC = JOINT ? N * (1 + K) : N;
-  return sqrtf(err2 * (1.0f / NC));  // err2 >= 0
-}
-
-struct Ctl {
-  float rtol, atol;
-  double hmax, hmin;
-  int64_t max_steps;
-  double escape;
-};
-
-// Integrates exactly `len` time units.  Returns 0 or a status code
-// (1 non-finite, 2 step underflow, 3 step budget exhausted, 4 escaped: a
-// state component left the ball of radius c.escape).
-template <class M, int K, class R, int INTEG, bool JOINT>
-CL_HD int integrate(PointState<M, K, R, INTEG> &st, double len, const Ctl &c) {
-  constexpr int N = M::N;
-  constexpr float safe = 0.9f, beta = 0.04f, facc1 = 5.0f, facc2 = 0.1f;
-  constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
-  double t = 0.0;
-  bool reject = false;
-  if (INTEG == kDopri5) {
-    M::f(st.x, st.kx, st.p);
-    if (JOINT) {
-#pragma unroll
-      for (int i = 0; i < K; i++) M::jv(st.V[i], st.kv[i], st.p, st.x);
-    }
-  }
-  while (t < len) {
-    if (st.steps >= c.max_steps) return 3;
-    if (!((double)st.h >= c.hmin)) return 2;  // also catches h == 0 and NaN
-    const double remaining = len - t;
-    const bool clamped = (double)st.h >= remaining;
-    const R h = clamped ? (R)remaining : st.h;
-    R x1[N], V1[K][N], kx1[N], kv1[K][N];
-    st.steps++;
-    const float err = attempt<M, K, R, INTEG, JOINT>(st, h, c.rtol, c.atol, x1, V1, kx1, kv1);
-    if (!(err == err) || err > 3.0e38f) return 1;
-    const float fac11 = exp2f(expo1 * fast_log2f(fmaxf(err, 1e-30f)));
-    float fac = fac11 * exp2f(-beta * fast_log2f(st.fac_old));
-    fac = fmaxf(facc2, fminf(facc1, fac * (1.0f / safe)));
-    R hnew = h * (R)fast_div(1.0f, fac);
-    if (err <= 1.0f) {
-      st.fac_old = fmaxf(err, 1e-4f);
-#pragma unroll
-      for (int j = 0; j < N; j++) {
-        st.x[j] = x1[j];
-        if (INTEG == kDopri5) st.kx[j] = kx1[j];
-      }
-      if (JOINT) {
-#pragma unroll
-        for (int i = 0; i < K; i++)
-#pragma unroll
-          for (int j = 0; j < N; j++) {
-            st.V[i][j] = V1[i][j];
-            if (INTEG == kDopri5) st.kv[i][j] = kv1[i][j];
-          }
-      }
-      if ((double)hnew > c.hmax) hnew = (R)c.hmax;
-      if (reject && hnew > h) hnew = h;
-      reject = false;
-      t = clamped ? len : t + (double)h;
-      if (!clamped || hnew < h) st.h = hnew;
-      bool inside = true;
-#pragma unroll
-      for (int j = 0; j < N; j++) inside = inside && (fabs(st.x[j]) <= (R)c.escape);
-      if (!inside) return 4;
-    } else {
-      st.h = h * (R)fast_div(1.0f, fminf(facc1, fac11 * (1.0f / safe)));
-      reject = true;
-    }
-  }
-  return 0;
+  const float inv_nc = joint ? 1.0f / (N * (1 + K)) : 1.0f / N;
+  return sqrtf(err2 * inv_nc);  // err2 >= 0
 }
 
 // Gram-Schmidt in FP64 on the k tangent vectors; r[i] = norms before scaling.
@@ -391,105 +347,219 @@ CL_HD void renormalise(R (&V)[K][N], double (&r)[K], int gs) {
     for (int j = 0; j < N; j++) V[i][j] = (R)v[i][j];
 }
 
-constexpr int kRenormSubInit = 16, kRenormSubMax = 64;
-
-// Largest log-norm spread allowed within one renormalisation sub-interval:
-// 0.3 ln(1 / max(rtol, unit roundoff of R)).
-template <class R> CL_HD float renorm_spread_limit(float rtol) {
-  const float ulp = sizeof(R) == 4 ? 5.96e-8f : 1.2e-16f;
-  return 0.3f * logf(1.0f / fmaxf(rtol, ulp));
+template <class M, int K, class R, int INTEG>
+CL_HD void refresh_tangent_derivs(Lane<M, K, R, INTEG> &L) {
+  if (INTEG == kDopri5) {
+#pragma unroll
+    for (int i = 0; i < K; i++) M::jv(L.V[i], L.kv[i], L.p, L.x);
+  }
 }
 
-// Whole per-point computation.  Returns the status code.
 template <class M, int K, class R, int INTEG>
-CL_HD int run_point(const AdaptiveArgs &a, int64_t pt) {
-  constexpr int N = M::N;
-  PointState<M, K, R, INTEG> st;
+CL_HD void lane_finish(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int status) {
 #pragma unroll
-  for (int i = 0; i < M::NP; i++) st.p[i] = (R)a.params.base[pt * a.params.ps + i * a.params.cs];
-#pragma unroll
-  for (int i = 0; i < N; i++) st.x[i] = (R)a.inits.base[pt * a.inits.ps + i * a.inits.cs];
-  st.h = (R)a.h0;
-  st.fac_old = 1e-4f;
-  st.steps = 0;
-  // A step below 1e-12 (model time units) is never meaningful here; it also
-  // stops a point whose controller collapsed the step to zero.
-  const Ctl c{(float)a.rtol, (float)a.atol, a.hmax > 0 ? a.hmax : 1e300, fmax(a.hmin, 1e-12),
-              a.max_steps, a.escape > 0 ? a.escape : 1e4};
-  const double t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
+  for (int i = 0; i < K; i++) {
+    const double lam = status ? quiet_nan() : L.sum[i] / L.t_avg;
+    a.spectrum.base[L.pt * a.spectrum.ps + i * a.spectrum.cs] = lam;
+  }
+  if (a.status) a.status[L.pt] = status;
+  if (a.steps) a.steps[L.pt] = L.steps;
+}
 
-  int status = 0;
-  if (a.t_transient > 0) status = integrate<M, K, R, INTEG, false>(st, a.t_transient, c);
+// Tangent basis = identity, start of the alignment / averaging phases.
+template <class M, int K, class R, int INTEG>
+CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
+  constexpr int N = M::N;
 #pragma unroll
   for (int i = 0; i < K; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) st.V[i][j] = (i == j) ? R(1) : R(0);
-  st.fac_old = 1e-4f;
-
-  double sum[K], comp[K];
-#pragma unroll
-  for (int i = 0; i < K; i++) sum[i] = comp[i] = 0.0;
-  const double total = a.t_align + t_avg;
-  const double eps_t = 1e-12 * total;
-  // Renormalisation sub-intervals.  The exponent estimate is the same for any
-  // renormalisation schedule (the R factors of successive Gram-Schmidt steps
-  // multiply to the R factor of the whole interval), but the weakest tangent
-  // direction is only resolved while its share of each tangent vector stays
-  // above the integration error.  So each dt_renorm interval is split into m
-  // equal parts, and m adapts per point to the spread of log-norms seen in one
-  // part: doubled when it exceeds tau, halved when below tau / 4.
-  const float tau = renorm_spread_limit<R>(c.rtol);
-  int m = kRenormSubInit;
-  double t = 0.0;
-  while (status == 0 && t < total) {
-    double len = a.dt_renorm;
-    if (t + len > total) len = total - t;
-    const double sub = len / m;
-    float max_spread = 0.f;
-    for (int j = 0; j < m; j++) {
-      const double l = (j == m - 1) ? len - sub * (m - 1) : sub;
-      status = integrate<M, K, R, INTEG, true>(st, l, c);
-      if (status) break;
-      double r[K];
-      renormalise<N, K, R>(st.V, r, a.gs);
-      bool ok = true;
-#pragma unroll
-      for (int i = 0; i < K; i++) ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
-      if (!ok) {
-        status = 1;
-        break;
-      }
-      double lg[K];
-      double lmax = -1e300, lmin = 1e300;
-#pragma unroll
-      for (int i = 0; i < K; i++) {
-        lg[i] = log(r[i]);
-        lmax = fmax(lmax, lg[i]);
-        lmin = fmin(lmin, lg[i]);
-      }
-      max_spread = fmaxf(max_spread, (float)(lmax - lmin));
-      if (t + sub * (j + 1) > a.t_align + eps_t) {
-#pragma unroll
-        for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
-          const double y = lg[i] - comp[i];
-          const double s2 = sum[i] + y;
-          comp[i] = (s2 - sum[i]) - y;
-          sum[i] = s2;
-        }
-      }
-    }
-    t += len;
-    if (max_spread > tau && m < kRenormSubMax) m *= 2;
-    else if (max_spread < 0.25f * tau && m > 1) m /= 2;
+    for (int j = 0; j < N; j++) L.V[i][j] = (i == j) ? R(1) : R(0);
+  refresh_tangent_derivs(L);
+  L.fac_old = 1e-4f;
+  L.t_phase = 0.0;
+  L.t_gs = 0.0;
+  if (a.t_align > 0) {
+    L.phase = kAlign;
+    L.phase_len = a.t_align;
+  } else {
+    L.phase = kAverage;
+    L.phase_len = L.t_avg;
   }
+}
+
+template <class M, int K, class R, int INTEG>
+CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt) {
+  constexpr int N = M::N;
+  L.pt = pt;
+#pragma unroll
+  for (int i = 0; i < M::NP; i++) L.p[i] = (R)a.params.base[pt * a.params.ps + i * a.params.cs];
+#pragma unroll
+  for (int i = 0; i < N; i++) L.x[i] = (R)a.inits.base[pt * a.inits.ps + i * a.inits.cs];
+  L.h = (R)a.h0;
+  L.fac_old = 1e-4f;
+  L.reject = false;
+  L.steps = 0;
+  L.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
+  L.L = a.dt_renorm / kRenormSplitInit;
+  L.rate_max = 0.0;
+#pragma unroll
+  for (int i = 0; i < K; i++) L.sum[i] = L.comp[i] = 0.0;
+  if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
+  if (a.t_transient > 0) {
+    L.phase = kTransient;
+    L.phase_len = a.t_transient;
+    L.t_phase = 0.0;
+    L.t_gs = 0.0;
+  } else {
+    lane_start_tangent(L, a);
+  }
+}
+
+// Gram-Schmidt step of one lane: log-norms accumulated in the averaging
+// phase, interval target adapted.  Returns false on a degenerate basis.
+template <class M, int K, class R, int INTEG>
+CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
+  double r[K];
+  renormalise<M::N, K, R>(L.V, r, a.gs);
+  double lmax = -1e300, lmin = 1e300;
+  bool ok = true;
+  double lg[K];
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    const double lam = status ? quiet_nan() : sum[i] / t_avg;
-    a.spectrum.base[pt * a.spectrum.ps + i * a.spectrum.cs] = lam;
+    ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
+    lg[i] = log(r[i]);
+    lmax = fmax(lmax, lg[i]);
+    lmin = fmin(lmin, lg[i]);
   }
-  if (a.status) a.status[pt] = status;
-  if (a.steps) a.steps[pt] = st.steps;
-  return status;
+  if (!ok) return false;
+  if (L.phase == kAverage) {
+#pragma unroll
+    for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
+      const double y = lg[i] - L.comp[i];
+      const double s = L.sum[i] + y;
+      L.comp[i] = (s - L.sum[i]) - y;
+      L.sum[i] = s;
+    }
+  }
+  if (L.t_gs > 0.0) {  // spread per unit time -> next interval
+    // The spread rate varies along an orbit (bursts of strong contraction),
+    // so the interval follows the largest recent rate, forgotten slowly.
+    const double rate = (lmax - lmin) / L.t_gs;
+    L.rate_max = fmax(rate, 0.995 * L.rate_max);
+    const double target = 0.5 * c.tau / fmax(L.rate_max, 1e-30);
+    L.L = fmin(a.dt_renorm, fmax(a.dt_renorm / kRenormSplitMax, target));
+  }
+  L.t_gs = 0.0;
+  refresh_tangent_derivs(L);
+  return true;
+}
+
+// One step attempt of one lane, phase bookkeeping included.  Returns
+// kFinished once the point's outputs are written.
+template <class M, int K, class R, int INTEG>
+CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
+  constexpr int N = M::N;
+  constexpr float safe = 0.9f, beta = 0.04f, facc1 = 5.0f, facc2 = 0.1f;
+  constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
+  if (L.steps >= c.max_steps) {
+    lane_finish(L, a, 3);
+    return kFinished;
+  }
+  if (!((double)L.h >= c.hmin)) {  // also catches h == 0 and NaN
+    lane_finish(L, a, 2);
+    return kFinished;
+  }
+  const double remaining = L.phase_len - L.t_phase;
+  const bool clamped = (double)L.h >= remaining;
+  const R h = clamped ? (R)remaining : L.h;
+  const bool joint = L.phase != kTransient;
+  R x1[N], V1[K][N], kx1[N], kv1[K][N];
+  L.steps++;
+  const float err = attempt<M, K, R, INTEG>(L, h, joint, c.rtol, c.atol, x1, V1, kx1, kv1);
+  if (!(err == err) || err > 3.0e38f) {
+    lane_finish(L, a, 1);
+    return kFinished;
+  }
+  const float fac11 = exp2f(expo1 * fast_log2f(fmaxf(err, 1e-30f)));
+  if (err <= 1.0f) {
+    float fac = fac11 * exp2f(-beta * fast_log2f(L.fac_old));
+    fac = fmaxf(facc2, fminf(facc1, fac * (1.0f / safe)));
+    R hnew = h * (R)fast_div(1.0f, fac);
+    L.fac_old = fmaxf(err, 1e-4f);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      L.x[j] = x1[j];
+      if (INTEG == kDopri5) L.kx[j] = kx1[j];
+    }
+    if (joint) {
+#pragma unroll
+      for (int i = 0; i < K; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+          L.V[i][j] = V1[i][j];
+          if (INTEG == kDopri5) L.kv[i][j] = kv1[i][j];
+        }
+    }
+    if ((double)hnew > c.hmax) hnew = (R)c.hmax;
+    if (L.reject && hnew > h) hnew = h;
+    L.reject = false;
+    if (!clamped || hnew < h) L.h = hnew;  // else keep the unclamped proposal
+    L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
+    L.t_gs += (double)h;
+    bool inside = true;
+#pragma unroll
+    for (int j = 0; j < N; j++) inside = inside && (fabs(L.x[j]) <= (R)c.escape);
+    if (!inside) {
+      lane_finish(L, a, 4);
+      return kFinished;
+    }
+    if (clamped) {  // landed on a phase end
+      if (L.phase == kTransient) {
+        lane_start_tangent(L, a);
+      } else if (L.phase == kAlign) {
+        if (!lane_gram_schmidt(L, a, c)) {
+          lane_finish(L, a, 1);
+          return kFinished;
+        }
+        L.phase = kAverage;
+        L.phase_len = L.t_avg;
+        L.t_phase = 0.0;
+      } else {
+        const bool ok = lane_gram_schmidt(L, a, c);
+        lane_finish(L, a, ok ? 0 : 1);
+        return kFinished;
+      }
+    }
+  } else {
+    L.h = h * (R)fast_div(1.0f, fminf(facc1, fac11 * (1.0f / safe)));
+    L.reject = true;
+  }
+  return kRunning;
+}
+
+template <class R>
+CL_HD Ctl make_ctl(const AdaptiveArgs &a) {
+  // A step below 1e-12 (model time units) is never meaningful here; it also
+  // stops a point whose controller collapsed the step to zero.
+  return Ctl{(float)a.rtol, (float)a.atol, renorm_spread_limit<R>((float)a.rtol),
+             a.hmax > 0 ? a.hmax : 1e300, fmax(a.hmin, 1e-12), a.max_steps,
+             a.escape > 0 ? a.escape : 1e4};
+}
+
+// One point start to finish on one thread (the host form of the kernel
+// loop, used by tests that run the integrator on the CPU).
+template <class M, int K, class R, int INTEG>
+CL_HD void run_point(const AdaptiveArgs &a, int64_t pt) {
+  const Ctl c = make_ctl<R>(a);
+  Lane<M, K, R, INTEG> L;
+  lane_start(L, a, pt);
+  for (;;) {
+    if (lane_step(L, a, c) == kFinished) return;
+    if (L.phase != kTransient && L.t_gs >= L.L && !lane_gram_schmidt(L, a, c)) {
+      lane_finish(L, a, 1);
+      return;
+    }
+  }
 }
 
 }  // namespace adaptive
