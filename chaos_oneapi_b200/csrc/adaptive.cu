@@ -29,8 +29,11 @@ __device__ __forceinline__ int64_t next_point(const AdaptiveArgs &a) {
 // the next one from the queue (persistent form) and carries on.  Gram-Schmidt
 // is voted per warp: when any lane is due, every lane past its transient
 // renormalises in the same pass.
-template <class M, int K, class R, int INTEG>
-__global__ void __launch_bounds__(128) sweep_kernel(const AdaptiveArgs a) {
+// MINB: resident 128-thread blocks per SM the kernel is compiled for (a
+// register cap: 4 -> 128 registers, 5 -> 96 with a few spills); the
+// autotuner picks the variant.
+template <class M, int K, class R, int INTEG, int MINB>
+__global__ void __launch_bounds__(128, MINB) sweep_kernel(const AdaptiveArgs a) {
   const Ctl c = make_ctl<R>(a);
   Lane<M, K, R, INTEG> L;
   int64_t pt = a.queue ? next_point(a) : (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,9 +58,12 @@ __global__ void __launch_bounds__(128) sweep_kernel(const AdaptiveArgs a) {
 }
 
 template <class M, class R, int INTEG>
-int launch_mri(const AdaptiveArgs &a, int block, int persistent_blocks, cudaStream_t s) {
+int launch_mri(const AdaptiveArgs &a, int block, int persistent_blocks, int variant,
+               cudaStream_t s) {
   if (a.k != M::N) return kErrUnsupported;
-  auto kern = sweep_kernel<M, M::N, R, INTEG>;
+  auto kern = sweep_kernel<M, M::N, R, INTEG, 1>;
+  if (sizeof(R) == 4) kern = variant == 1 ? sweep_kernel<M, M::N, R, INTEG, 5>
+                                          : sweep_kernel<M, M::N, R, INTEG, 4>;
   unsigned grid;
   if (a.queue) {
     if (persistent_blocks <= 0) {
@@ -78,13 +84,14 @@ int launch_mri(const AdaptiveArgs &a, int block, int persistent_blocks, cudaStre
 }
 
 template <class M>
-int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks, cudaStream_t s) {
+int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks, int variant,
+             cudaStream_t s) {
   if (integ == kDverk65) {
-    if (prec == kFP64) return launch_mri<M, double, kDverk65>(a, block, pblocks, s);
-    if (prec == kFP32) return launch_mri<M, float, kDverk65>(a, block, pblocks, s);
+    if (prec == kFP64) return launch_mri<M, double, kDverk65>(a, block, pblocks, variant, s);
+    if (prec == kFP32) return launch_mri<M, float, kDverk65>(a, block, pblocks, variant, s);
   } else if (integ == kDopri5) {
-    if (prec == kFP64) return launch_mri<M, double, kDopri5>(a, block, pblocks, s);
-    if (prec == kFP32) return launch_mri<M, float, kDopri5>(a, block, pblocks, s);
+    if (prec == kFP64) return launch_mri<M, double, kDopri5>(a, block, pblocks, variant, s);
+    if (prec == kFP32) return launch_mri<M, float, kDopri5>(a, block, pblocks, variant, s);
   }
   return kErrUnsupported;
 }
@@ -92,16 +99,17 @@ int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks,
 }  // namespace adaptive
 
 int launch_adaptive(int model, int integ, int prec, const AdaptiveArgs &a, int block,
-                    int persistent_blocks, cudaStream_t s) {
+                    int persistent_blocks, int variant, cudaStream_t s) {
   using namespace adaptive;
   if (a.P <= 0) return 0;
-  if (block <= 0 || block > 128) block = 128;
+  if (block <= 0 || block > 128 || block % 32) block = 128;
+  const int pb = persistent_blocks, v = variant;
   switch (model) {
-    case kShimizu: return launch_m<Shimizu>(integ, prec, a, block, persistent_blocks, s);
-    case kLorenz: return launch_m<Lorenz>(integ, prec, a, block, persistent_blocks, s);
-    case kRossler: return launch_m<Rossler>(integ, prec, a, block, persistent_blocks, s);
-    case kChua: return launch_m<Chua>(integ, prec, a, block, persistent_blocks, s);
-    case kHyperRossler: return launch_m<HyperRossler>(integ, prec, a, block, persistent_blocks, s);
+    case kShimizu: return launch_m<Shimizu>(integ, prec, a, block, pb, v, s);
+    case kLorenz: return launch_m<Lorenz>(integ, prec, a, block, pb, v, s);
+    case kRossler: return launch_m<Rossler>(integ, prec, a, block, pb, v, s);
+    case kChua: return launch_m<Chua>(integ, prec, a, block, pb, v, s);
+    case kHyperRossler: return launch_m<HyperRossler>(integ, prec, a, block, pb, v, s);
     default: return kErrUnsupported;
   }
 }

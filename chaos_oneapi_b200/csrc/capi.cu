@@ -95,6 +95,7 @@ struct chaos_lyap_handle {
   int sm_count = 0;
   int block = 0;
   int schedule = CHAOS_SCHED_PERSISTENT;
+  int variant = 0;  // register-cap variant of the FP32 kernels (autotuned)
   cudaStream_t own_stream = nullptr;
   cudaStream_t last_stream = nullptr;
   unsigned long long *queue = nullptr;  // persistent-schedule point counter
@@ -227,6 +228,7 @@ int chaos_lyap_create(const chaos_lyap_desc *desc, chaos_lyap_handle **out) {
   cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, d.device);
   h->block = d.block > 0 ? d.block : (d.precision == CHAOS_PREC_COMPAT_FP64 ? 64 : 128);
   h->schedule = d.schedule == CHAOS_SCHED_DIRECT ? CHAOS_SCHED_DIRECT : CHAOS_SCHED_PERSISTENT;
+  h->variant = d.variant == 1 ? 1 : 0;
   if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
     delete h;
     return cuda_fail(e, "cudaStreamCreate");
@@ -266,7 +268,7 @@ int chaos_lyap_destroy(chaos_lyap_handle *h) {
 
 static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double *inits,
                    double *spectrum, int32_t *status, int64_t *steps, const double *tavg,
-                   cudaStream_t s, int block, int schedule, double t_avg_override,
+                   cudaStream_t s, int block, int schedule, int variant, double t_avg_override,
                    double t_transient_override) {
   const chaos_lyap_desc &d = h->d;
   const ModelInfo *m = h->model;
@@ -320,9 +322,9 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
       if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
       a.queue = h->queue;
       a.queue_stride = chaos::queue_stride_for(P);
-      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);
+      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
     } else {
-      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, s);
+      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
     }
   }
   if (rc == chaos::kErrUnsupported)
@@ -343,7 +345,7 @@ int chaos_lyap_run(chaos_lyap_handle *h, int64_t P, const double *params, double
   DeviceGuard g(h->d.device);
   if (!g.ok) return fail(CHAOS_LYAP_ECUDA, "cannot select device %d", h->d.device);
   return enqueue(h, P, params, inits, spectrum, status, steps, tavg, (cudaStream_t)stream, h->block,
-                 h->schedule, -1.0, -1.0);
+                 h->schedule, h->variant, -1.0, -1.0);
 }
 
 int chaos_lyap_sync(chaos_lyap_handle *h) {
@@ -392,7 +394,7 @@ int chaos_lyap_run_host(chaos_lyap_handle *h, int64_t P, const double *params, d
     return cuda_fail(e, "copy in");
   int rc = enqueue(h, P, h->s_params, h->s_inits, h->s_spec, status ? h->s_status : nullptr,
                    steps ? h->s_steps : nullptr, tavg ? h->s_tavg : nullptr, s, h->block,
-                   h->schedule, -1.0, -1.0);
+                   h->schedule, h->variant, -1.0, -1.0);
   if (rc) return rc;
   if ((e = cudaMemcpyAsync(spectrum, h->s_spec, bs, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_fail(e, "copy out");
@@ -430,37 +432,47 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int blocks[] = {32, 64, 128};
+  const int blocks[] = {64, 128};
   const int scheds[] = {CHAOS_SCHED_DIRECT, CHAOS_SCHED_PERSISTENT};
+  const int nvar = h->d.precision == CHAOS_PREC_FP32 ? 2 : 1;
   float best = 1e30f;
-  int best_b = h->block, best_s = h->schedule, rc = CHAOS_LYAP_OK;
+  int best_b = h->block, best_s = h->schedule, best_v = h->variant, rc = CHAOS_LYAP_OK;
   cudaStream_t s = h->own_stream;
-  for (int b : blocks)
-    for (int sc : scheds) {
-      float ms = 0;
-      for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
-        cudaEventRecord(e0, s);
-        rc = enqueue(h, sample, params, const_cast<double *>(inits), spec, nullptr, nullptr,
-                     nullptr, s, b, sc, t_avg, t_tr);
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
-        cudaEventElapsedTime(&ms, e0, e1);  // second repetition is the warm one
+  for (int v = 0; v < nvar && rc == CHAOS_LYAP_OK; v++)
+    for (int b : blocks)
+      for (int sc : scheds) {
+        float ms = 0;
+        for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
+          cudaEventRecord(e0, s);
+          rc = enqueue(h, sample, params, const_cast<double *>(inits), spec, nullptr, nullptr,
+                       nullptr, s, b, sc, v, t_avg, t_tr);
+          cudaEventRecord(e1, s);
+          cudaEventSynchronize(e1);
+          cudaEventElapsedTime(&ms, e0, e1);  // second repetition is the warm one
+        }
+        if (rc) break;
+        if (ms < best) {
+          best = ms;
+          best_b = b;
+          best_s = sc;
+          best_v = v;
+        }
       }
-      if (rc) break;
-      if (ms < best) {
-        best = ms;
-        best_b = b;
-        best_s = sc;
-      }
-    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(spec);
   if (rc) return rc;
   h->block = best_b;
   h->schedule = best_s;
+  h->variant = best_v;
   if (block_out) *block_out = best_b;
   if (schedule_out) *schedule_out = best_s;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant) {
+  if (!h || !variant) return fail(CHAOS_LYAP_EINVAL, "null argument");
+  *variant = h->variant;
   return CHAOS_LYAP_OK;
 }
 

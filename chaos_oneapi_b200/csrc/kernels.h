@@ -71,8 +71,9 @@ enum Precision : int32_t { kCompatFP64 = 0, kFP64 = 1, kFP32 = 2 };
 constexpr int kErrUnsupported = -1;
 
 int launch_compat(int model, const CompatArgs &a, int block, cudaStream_t s);
+// variant: 0 = 128-register build, 1 = 96-register build (FP32 only)
 int launch_adaptive(int model, int integrator, int precision, const AdaptiveArgs &a, int block,
-                    int persistent_blocks, cudaStream_t s);
+                    int persistent_blocks, int variant, cudaStream_t s);
 int launch_l96_warp(int integrator, int precision, const AdaptiveArgs &a, int warps_per_block,
                     cudaStream_t s);
 

@@ -46,7 +46,7 @@ class Desc(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("schedule", ctypes.c_int32),
         ("block", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("variant", ctypes.c_int32),
         ("escape", ctypes.c_double),
         ("reserved", ctypes.c_int32 * 4),
     ]
@@ -81,6 +81,7 @@ SIGNATURES = {
     "chaos_lyap_autotune": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P,
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
+    "chaos_lyap_get_variant": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "chaos_lyap_cudaLyapunov": (ctypes.c_int, [
         ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         _P, _P, ctypes.c_int32, ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_double,

@@ -87,6 +87,7 @@ class SweepConfig:
     device: int = 0
     schedule: str = "auto"       # auto | direct | persistent
     block: int = 0
+    variant: int = 0
     extra: dict = field(default_factory=dict)
 
     def to_desc(self) -> Desc:
@@ -108,6 +109,7 @@ class SweepConfig:
         d.device = self.device
         d.schedule = native.SCHED[self.schedule]
         d.block = self.block
+        d.variant = self.variant
         return d
 
 
@@ -203,7 +205,13 @@ class Sweep:
         b, s = ctypes.c_int32(), ctypes.c_int32()
         check(lib.chaos_lyap_autotune(self._h, sample, _tptr(params, "float64"),
                                       _tptr(inits, "float64"), ctypes.byref(b), ctypes.byref(s)))
-        return {"block": b.value, "schedule": {1: "direct", 2: "persistent"}.get(s.value, "auto")}
+        return {"block": b.value, "schedule": {1: "direct", 2: "persistent"}.get(s.value, "auto"),
+                "variant": self.variant_in_use()}
+
+    def variant_in_use(self) -> int:
+        v = ctypes.c_int32()
+        check(lib.chaos_lyap_get_variant(self._h, ctypes.byref(v)))
+        return v.value
 
 
 def cuda_lyapunov(task_num, is_qr, is_var, inits, close_points, dimension, model, params,

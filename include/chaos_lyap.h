@@ -97,7 +97,8 @@ typedef struct chaos_lyap_desc {
   int32_t device;           /* CUDA device ordinal */
   int32_t schedule;         /* CHAOS_SCHED_* */
   int32_t block;            /* threads per block, 0 = tuned default */
-  int32_t reserved0;
+  int32_t variant;          /* FP32 kernels: 0 = 128-register build, 1 = 96-register
+                               build (more resident warps, a few spills); autotuned */
   double escape;            /* adaptive: escape radius of the state (0: 1e4) */
   int32_t reserved[4];
 } chaos_lyap_desc;
@@ -162,6 +163,9 @@ int chaos_lyap_sync(chaos_lyap_handle *h);
  * block size in *block_out and schedule in *schedule_out when non-null. */
 int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
                         const double *inits, int32_t *block_out, int32_t *schedule_out);
+
+/* The FP32 kernel variant in use (desc.variant, or the autotuner's choice). */
+int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);
 
 /* Drop-in for the reference launcher cudaLyapunov (cuda/lyapunov.dp.hpp:10-17)
  * with the same argument meaning, DEVICE pointers, point-major layout:
