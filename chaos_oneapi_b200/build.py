@@ -40,7 +40,8 @@ CUDA_UNITS = {
     "peak.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]
-HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp"]
+HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp",
+              "host_capi.cpp"]
 
 
 def nvcc() -> str:
@@ -69,7 +70,8 @@ def _deps_mtime(dirs) -> float:
         for f in os.listdir(d):
             if f.endswith((".h", ".cuh", ".hpp")):
                 t = max(t, os.path.getmtime(os.path.join(d, f)))
-    t = max(t, os.path.getmtime(os.path.join(ROOT, "include", "chaos_lyap.h")))
+    for h in ("chaos_lyap.h", "chaos_lyap_host.h"):
+        t = max(t, os.path.getmtime(os.path.join(ROOT, "include", h)))
     return t
 
 
@@ -113,7 +115,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         obj = os.path.join(BUILD, "host_" + unit + ".o")
         host_objs.append(obj)
         if force or _stale(obj, src, dep_t):
-            jobs_list.append(["g++"] + CXX_FLAGS + ["-I" + jinc, "-c", src, "-o", obj])
+            jobs_list.append(["g++"] + CXX_FLAGS + ["-I" + jinc, "-I" + HOST, "-c", src, "-o", obj])
     with ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
         for out in ex.map(_run, jobs_list):
             if verbose and out.strip():
@@ -125,8 +127,8 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
     main_src = os.path.join(HOST, "main.cpp")
     if os.path.exists(main_src) and (force or not os.path.exists(CLI)
                                      or os.path.getmtime(CLI) < max(newest, os.path.getmtime(main_src))):
-        _run(["g++"] + CXX_FLAGS + ["-I" + jinc, main_src, "-o", CLI, "-L" + PKG, "-lchaos_lyap",
-                                    "-Wl,-rpath,$ORIGIN"])
+        _run(["g++"] + CXX_FLAGS + ["-I" + jinc, "-I" + HOST, main_src, "-o", CLI, "-L" + PKG,
+                                    "-l:libchaos_lyap.so", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

@@ -37,7 +37,45 @@ def case_inputs(model, seed=7):
     return params, inits
 
 
+# The reference program itself (main.cpp: config.json -> Data/Lyapunov
+# shimizu.json), run on a small Shimizu-Morioka map for each method.
+PROGRAM_CFG = {
+    "hardware": {"num_GPUs": 1},
+    "tool": {"lyapunov": {"samples_num": 1, "using_qr": False, "using_var": True}},
+    "systems": [{
+        "model_name": "shimizu", "lyapunov_exponent_num": 3, "epsilon": 1e-7,
+        "integration_step": 1e-2, "skip_time_attractor": 20.0,
+        "skip_time_slave_trajectory": 5.0, "skip_time_normalization": 0.5, "total_time": 50.0,
+        "initial_state": [1e-4, 0, 0], "initial_model_params": [0, 0],
+        "first_sweep_param": [0, 0.2, 2, 6], "second_sweep_param": [1, 0, 1.2, 5]}],
+}
+
+
+def program_outputs():
+    import json
+    import shutil
+    import subprocess
+    import tempfile
+    for method, (qr, var) in {"fd": (False, False), "var": (False, True), "qr": (True, False)}.items():
+        cfg = json.loads(json.dumps(PROGRAM_CFG))
+        cfg["tool"]["lyapunov"].update(using_qr=qr, using_var=var)
+        d = tempfile.mkdtemp()
+        try:
+            os.mkdir(os.path.join(d, "Data"))
+            with open(os.path.join(d, "config.json"), "w") as f:
+                json.dump(cfg, f, indent=2)
+            subprocess.run([oracle.REF_MAIN], cwd=d, check=True, capture_output=True,
+                           env=dict(os.environ, CHAOS_REF_THREADS="4"))
+            shutil.copy(os.path.join(d, "config.json"),
+                        os.path.join(HERE, f"program_{method}_config.json"))
+            shutil.copy(os.path.join(d, "Data", "Lyapunov shimizu.json"),
+                        os.path.join(HERE, f"program_{method}_output.json"))
+        finally:
+            shutil.rmtree(d)
+
+
 def main():
+    program_outputs()
     out = {}
     for model, (pb, xb, k, h, ts, tc, tt, dn) in CASES.items():
         params, inits = case_inputs(model)
