@@ -315,17 +315,14 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
     a.steps = steps;
     const int integ = d.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
     const int prec = d.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
-    if (m->dim > 4) {
-      rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
-    } else if (schedule == CHAOS_SCHED_PERSISTENT) {
+    if (schedule == CHAOS_SCHED_PERSISTENT) {
       cudaError_t e = cudaMemsetAsync(h->queue, 0, sizeof(unsigned long long), s);
       if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
       a.queue = h->queue;
       a.queue_stride = chaos::queue_stride_for(P);
-      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
-    } else {
-      rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
     }
+    if (m->dim > 4) rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
+    else rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
   }
   if (rc == chaos::kErrUnsupported)
     return fail(CHAOS_LYAP_EUNSUPPORTED, "no kernel for model %s with this integrator/precision/k",

@@ -1,8 +1,527 @@
-// Warp-per-point sweep for the 40-dimensional Lorenz-96 model.
+// Warp-per-point sweep for the 40-dimensional Lorenz-96 model
+//   x_i' = (x_{i+1} - x_{i-2}) x_{i-1} - gamma x_i + F   (cyclic)
+// with its k <= 40 tangent vectors: Dormand-Prince 5(4) in FP32, modified
+// Gram-Schmidt QR in FP64, log-norms in FP64.
+//
+// Layout.  One warp owns one point.  Its 32 lanes form 4 groups of 8; a group
+// holds one 40-vector, 5 consecutive components per lane, so the stencil's
+// neighbours i-2, i-1, i+1 are in the lane except at its edges, where 3
+// shuffles per stage fetch them from the adjacent lanes (cyclically within
+// the group).  A step runs the state first (every group computes it, so each
+// lane has the stage points it needs for J without any exchange), then the k
+// tangent vectors four at a time.  Per-step registers: the lane's 5
+// components of the 7 stage points as Jacobian coefficients, plus one
+// vector's Dopri5 stages.  Between steps the tangent vectors and their FSAL
+// derivatives live in shared memory (double-buffered: candidate / accepted),
+// 4 x k x 40 floats per warp; the FP64 QR reuses the candidate half.
+//
+// The phase and renormalisation logic follows adaptive.cuh (transient /
+// alignment / averaging with clamped landings, interval from the
+// Gram-Schmidt cancellation factor, norm products flushed into Kahan sums,
+// escape radius, step budget); every decision is warp-uniform.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace chaos {
+namespace l96 {
 
-int launch_l96_warp(int, int, const AdaptiveArgs &, int, cudaStream_t) { return kErrUnsupported; }
+constexpr int N = 40;        // model dimension
+constexpr int G = 4;         // vectors processed at once per warp (lane groups)
+constexpr int C = 5;         // components per lane
+constexpr int WARPS = 8;     // warps (points) per block
+constexpr unsigned FULL = 0xffffffffu;
+
+struct DPc {  // Dormand-Prince 5(4), cuda/tools/dopri.dp.cpp:14-44
+  static constexpr float a21 = 0.2f;
+  static constexpr float a31 = 3.f / 40.f, a32 = 9.f / 40.f;
+  static constexpr float a41 = 44.f / 45.f, a42 = -56.f / 15.f, a43 = 32.f / 9.f;
+  static constexpr float a51 = 19372.f / 6561.f, a52 = -25360.f / 2187.f, a53 = 64448.f / 6561.f,
+                         a54 = -212.f / 729.f;
+  static constexpr float a61 = 9017.f / 3168.f, a62 = -355.f / 33.f, a63 = 46732.f / 5247.f,
+                         a64 = 49.f / 176.f, a65 = -5103.f / 18656.f;
+  static constexpr float b1 = 35.f / 384.f, b3 = 500.f / 1113.f, b4 = 125.f / 192.f,
+                         b5 = -2187.f / 6784.f, b6 = 11.f / 84.f;
+  static constexpr float e1 = 71.f / 57600.f, e3 = -71.f / 16695.f, e4 = 71.f / 1920.f,
+                         e5 = -17253.f / 339200.f, e6 = 22.f / 525.f, e7 = -1.f / 40.f;
+};
+
+// Neighbour fetch within the lane's group: left lane's components 3, 4 and
+// the right lane's component 0.
+struct Nb {
+  float l3, l4, r0;
+};
+__device__ __forceinline__ Nb neighbours(const float (&v)[C], int left, int right) {
+  Nb n;
+  n.l3 = __shfl_sync(FULL, v[3], left);
+  n.l4 = __shfl_sync(FULL, v[4], left);
+  n.r0 = __shfl_sync(FULL, v[0], right);
+  return n;
+}
+// Extended window w[-2..5] of the lane's components: at(j) = w[j] for j in -2..5.
+struct Win {
+  float w[C + 3];
+  __device__ __forceinline__ float at(int j) const { return w[j + 2]; }
+};
+__device__ __forceinline__ Win window(const float (&v)[C], const Nb &n) {
+  Win e;
+  e.w[0] = n.l3;
+  e.w[1] = n.l4;
+#pragma unroll
+  for (int j = 0; j < C; j++) e.w[j + 2] = v[j];
+  e.w[C + 2] = n.r0;
+  return e;
+}
+
+// Jacobian coefficients of one stage point for the lane's components:
+// (J v)_i = (v_{i+1} - v_{i-2}) A_i + B_i v_{i-1} - gamma v_i,
+// A_i = x_{i-1}, B_i = x_{i+1} - x_{i-2}.
+struct Jc {
+  float A[C], B[C];
+};
+
+__device__ __forceinline__ void rhs_state(const float (&x)[C], float (&dx)[C], Jc &jc, float F,
+                                          float gam, int left, int right) {
+  const Win e = window(x, neighbours(x, left, right));
+#pragma unroll
+  for (int j = 0; j < C; j++) {
+    jc.A[j] = e.at(j - 1);
+    jc.B[j] = e.at(j + 1) - e.at(j - 2);
+    dx[j] = jc.B[j] * jc.A[j] - gam * e.at(j) + F;
+  }
+}
+
+__device__ __forceinline__ void rhs_tangent(const float (&v)[C], float (&dv)[C], const Jc &jc,
+                                            float gam, int left, int right) {
+  const Win e = window(v, neighbours(v, left, right));
+#pragma unroll
+  for (int j = 0; j < C; j++)
+    dv[j] = (e.at(j + 1) - e.at(j - 2)) * jc.A[j] + jc.B[j] * e.at(j - 1) - gam * e.at(j);
+}
+
+__device__ __forceinline__ float err_term(float y0, float y1, float e, float rtol, float atol) {
+  const float m = fmaxf(fabsf(y0), fabsf(y1));
+  const float r = __fdividef(e, fmaf(rtol, m, atol));
+  return r * r;
+}
+
+// One Dopri5 pass over the lane's 5 components.  rhs(s, arg, out) evaluates
+// stage s (1..6; stage 0 = k1 is given) at arg.
+template <class RHS>
+__device__ __forceinline__ void dopri_pass(const float (&y)[C], const float (&k1)[C], float h,
+                                           const RHS &rhs, float (&y1)[C], float (&k7)[C],
+                                           float &err2, float rtol, float atol) {
+  using T = DPc;
+  float k2[C], k3[C], k4[C], k5[C], arg[C], e[C];
+#pragma unroll
+  for (int j = 0; j < C; j++) arg[j] = y[j] + h * (T::a21 * k1[j]);
+  rhs(1, arg, k2);
+#pragma unroll
+  for (int j = 0; j < C; j++) arg[j] = y[j] + h * (T::a31 * k1[j] + T::a32 * k2[j]);
+  rhs(2, arg, k3);
+#pragma unroll
+  for (int j = 0; j < C; j++) arg[j] = y[j] + h * (T::a41 * k1[j] + T::a42 * k2[j] + T::a43 * k3[j]);
+  rhs(3, arg, k4);
+#pragma unroll
+  for (int j = 0; j < C; j++)
+    arg[j] = y[j] + h * (T::a51 * k1[j] + T::a52 * k2[j] + T::a53 * k3[j] + T::a54 * k4[j]);
+  rhs(4, arg, k5);
+#pragma unroll
+  for (int j = 0; j < C; j++) {
+    arg[j] = y[j] + h * (T::a61 * k1[j] + T::a62 * k2[j] + T::a63 * k3[j] + T::a64 * k4[j] +
+                         T::a65 * k5[j]);
+    e[j] = T::e1 * k1[j] + T::e3 * k3[j] + T::e4 * k4[j] + T::e5 * k5[j];
+    y1[j] = T::b1 * k1[j] + T::b3 * k3[j] + T::b4 * k4[j] + T::b5 * k5[j];
+  }
+  {
+    float k6[C];
+    rhs(5, arg, k6);
+#pragma unroll
+    for (int j = 0; j < C; j++) {
+      y1[j] = y[j] + h * (y1[j] + T::b6 * k6[j]);
+      e[j] += T::e6 * k6[j];
+    }
+  }
+  rhs(6, y1, k7);
+#pragma unroll
+  for (int j = 0; j < C; j++) {
+    e[j] += T::e7 * k7[j];
+    err2 += err_term(y[j], y1[j], h * e[j], rtol, atol);
+  }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+__device__ __forceinline__ double group_sum(double v) {  // over the 8 lanes of a group
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+enum Phase : int { kTransient = 0, kAlign = 1, kAverage = 2 };
+
+struct Warp {
+  // per lane
+  float x[C], kx[C];
+  double sum[2], comp[2], prod[2];  // exponents lane and lane + 32
+  // warp-uniform
+  float F, gam, h, fac_old;
+  bool reject;
+  int phase;
+  double t_phase, phase_len, t_gs, L, rate_max, t_avg;
+  long long steps;
+  long long pt;
+};
+
+__device__ __forceinline__ void flush_logs(Warp &w) {
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const double y = log(w.prod[i]) - w.comp[i];
+    const double s = w.sum[i] + y;
+    w.comp[i] = (s - w.sum[i]) - y;
+    w.sum[i] = s;
+    w.prod[i] = 1.0;
+  }
+}
+
+// Tangent FSAL derivatives KV = J(x) V for the k vectors.
+__device__ void refresh_kv(const Warp &w, const float *V, float *KV, int k, int g, int li,
+                           int left, int right) {
+  float dx[C];
+  Jc jc;
+  rhs_state(w.x, dx, jc, w.F, w.gam, left, right);
+  for (int r = 0; r < (k + G - 1) / G; r++) {
+    const int vec = r * G + g;
+    const bool valid = vec < k;
+    float v[C], dv[C];
+#pragma unroll
+    for (int j = 0; j < C; j++) v[j] = valid ? V[vec * N + li * C + j] : 0.f;
+    rhs_tangent(v, dv, jc, w.gam, left, right);
+    if (valid)
+#pragma unroll
+      for (int j = 0; j < C; j++) KV[vec * N + li * C + j] = dv[j];
+  }
+  __syncwarp();
+}
+
+// Modified Gram-Schmidt in FP64 on the k vectors of V (k x 40, FP32), through
+// the FP64 work area W (k x 40 doubles).  Returns max |v_q|^2 / r_q^2 (the
+// cancellation factor) and multiplies r_q into the lane that owns exponent q.
+__device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int lane,
+                         bool accumulate, bool &ok) {
+  // FP32 -> FP64, and squared norms before orthogonalisation
+  for (int idx = lane; idx < k * N; idx += 32) W[idx] = (double)V[idx];
+  __syncwarp();
+  double cancel = 1.0;
+  ok = true;
+  for (int q = 0; q < k; q++) {
+    double wq[C];
+#pragma unroll
+    for (int j = 0; j < C; j++) wq[j] = W[q * N + li * C + j];
+    double s = 0;
+#pragma unroll
+    for (int j = 0; j < C; j++) s = fma(wq[j], wq[j], s);
+    s = group_sum(s);
+    const double inv = rsqrt(s);
+    const double r = s * inv;
+    ok = ok && (r > 0.0) && (r < 1e300);
+#pragma unroll
+    for (int j = 0; j < C; j++) wq[j] *= inv;
+    __syncwarp();
+    if (g == 0) {
+#pragma unroll
+      for (int j = 0; j < C; j++) W[q * N + li * C + j] = wq[j];
+    }
+    // projections of the later vectors, four at a time
+    for (int j0 = q + 1; j0 < k; j0 += G) {
+      const int vj = j0 + g;
+      const bool valid = vj < k;
+      double wj[C];
+#pragma unroll
+      for (int j = 0; j < C; j++) wj[j] = valid ? W[vj * N + li * C + j] : 0.0;
+      double c = 0;
+#pragma unroll
+      for (int j = 0; j < C; j++) c = fma(wq[j], wj[j], c);
+      c = group_sum(c);
+      if (valid)
+#pragma unroll
+        for (int j = 0; j < C; j++) W[vj * N + li * C + j] = fma(-c, wq[j], wj[j]);
+    }
+    __syncwarp();
+    if (ok) {
+      // cancellation: norm before any projection vs r (the first vector has none)
+      if (q > 0) {
+        double b = 0;
+#pragma unroll
+        for (int j = 0; j < C; j++) {
+          const double vb = (double)V[q * N + li * C + j];
+          b = fma(vb, vb, b);
+        }
+        b = group_sum(b);
+        cancel = fmax(cancel, b / s);
+      }
+      if (accumulate && (q & 31) == lane) {
+        const int slot = q >> 5;
+        w.prod[slot] *= r;
+      }
+    }
+  }
+  __syncwarp();
+  for (int idx = lane; idx < k * N; idx += 32) V[idx] = (float)W[idx];
+  __syncwarp();
+  return cancel;
+}
+
+__device__ void finish(Warp &w, const AdaptiveArgs &a, int k, int lane, int status) {
+  flush_logs(w);
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const int q = lane + 32 * i;
+    if (q < k) {
+      const double lam = status ? __longlong_as_double(0x7ff8000000000000ULL) : w.sum[i] / w.t_avg;
+      a.spectrum.base[w.pt * a.spectrum.ps + q * a.spectrum.cs] = lam;
+    }
+  }
+  if (lane == 0) {
+    if (a.status) a.status[w.pt] = status;
+    if (a.steps) a.steps[w.pt] = w.steps;
+  }
+}
+
+__device__ __forceinline__ long long fetch(const AdaptiveArgs &a, int lane, long long direct) {
+  if (!a.queue) return direct;
+  unsigned long long q = 0;
+  if (lane == 0) q = atomicAdd(a.queue, 1ULL);
+  q = __shfl_sync(FULL, q, 0);
+  if (q >= (unsigned long long)a.P) return a.P;
+  return (long long)((q * (unsigned long long)a.queue_stride) % (unsigned long long)a.P);
+}
+
+__global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int g = lane >> 3, li = lane & 7;
+  const int left = g * 8 + ((li + 7) & 7), right = g * 8 + ((li + 1) & 7);
+  const int k = a.k;
+  const size_t per_warp = (size_t)4 * k * N;  // floats: V, KV, V1, KV1
+  float *base = reinterpret_cast<float *>(smem) + wid * per_warp;
+  float *V = base, *KV = base + k * N, *V1 = base + 2 * k * N, *KV1 = base + 3 * k * N;
+  double *W = reinterpret_cast<double *>(V1);  // FP64 QR work area (V1 + KV1)
+
+  const float rtol = (float)a.rtol, atol = (float)a.atol;
+  const float tau = 0.3f * logf(1.0f / fmaxf(rtol, 5.96e-8f));
+  const double hmax = a.hmax > 0 ? a.hmax : 1e300, hmin = fmax(a.hmin, 1e-12);
+  const float esc = (float)(a.escape > 0 ? a.escape : 1e4);
+  constexpr float safe = 0.9f, beta = 0.04f, facc1 = 5.0f, facc2 = 0.1f;
+  constexpr float expo1 = 0.2f - beta * 0.75f;
+
+  Warp w;
+  long long direct = (long long)blockIdx.x * WARPS + wid;
+  w.pt = fetch(a, lane, direct);
+
+  auto start_tangent = [&]() {
+    for (int idx = lane; idx < k * N; idx += 32) V[idx] = (idx / N == idx % N) ? 1.f : 0.f;
+    __syncwarp();
+    refresh_kv(w, V, KV, k, g, li, left, right);
+    w.fac_old = 1e-4f;
+    w.t_phase = 0.0;
+    w.t_gs = 0.0;
+    if (a.t_align > 0) {
+      w.phase = kAlign;
+      w.phase_len = a.t_align;
+    } else {
+      w.phase = kAverage;
+      w.phase_len = w.t_avg;
+    }
+  };
+  auto start_point = [&]() {
+    w.F = (float)a.params.base[w.pt * a.params.ps + 0 * a.params.cs];
+    w.gam = (float)a.params.base[w.pt * a.params.ps + 1 * a.params.cs];
+#pragma unroll
+    for (int j = 0; j < C; j++) w.x[j] = (float)a.inits.base[w.pt * a.inits.ps + (li * C + j) * a.inits.cs];
+    w.h = (float)a.h0;
+    w.fac_old = 1e-4f;
+    w.reject = false;
+    w.steps = 0;
+    w.t_avg = a.t_avg_per_point ? a.t_avg_per_point[w.pt] : a.t_avg;
+    w.L = a.dt_renorm / 16;
+    w.rate_max = 0.0;
+#pragma unroll
+    for (int i = 0; i < 2; i++) w.sum[i] = w.comp[i] = 0.0, w.prod[i] = 1.0;
+    Jc jc;
+    rhs_state(w.x, w.kx, jc, w.F, w.gam, left, right);
+    if (a.t_transient > 0) {
+      w.phase = kTransient;
+      w.phase_len = a.t_transient;
+      w.t_phase = 0.0;
+      w.t_gs = 0.0;
+    } else {
+      start_tangent();
+    }
+  };
+  // Gram-Schmidt of the warp's point; false on a degenerate basis.
+  auto gram_schmidt = [&]() -> bool {
+    bool ok;
+    const double cancel = mgs_qr(w, V, W, k, g, li, lane, w.phase == kAverage, ok);
+    if (!ok) return false;
+    if (w.phase == kAverage) {
+      bool fl = false;
+#pragma unroll
+      for (int i = 0; i < 2; i++) fl = fl || !(w.prod[i] < 1e150 && w.prod[i] > 1e-150);
+      if (__any_sync(FULL, fl)) flush_logs(w);
+    }
+    if (w.t_gs > 0.0) {
+      const double rate = 0.5 * (double)logf((float)cancel) / w.t_gs;
+      w.rate_max = fmax(rate, 0.995 * w.rate_max);
+      const double target = 0.125 * tau / fmax(w.rate_max, 1e-30);
+      w.L = fmin(a.dt_renorm, fmax(a.dt_renorm / 64, target));
+    }
+    w.t_gs = 0.0;
+    refresh_kv(w, V, KV, k, g, li, left, right);
+    return true;
+  };
+
+  if (w.pt < a.P) start_point();
+  while (w.pt < a.P) {
+    int status = -1;  // -1: running
+    if (w.steps >= a.max_steps) status = 3;
+    else if (!((double)w.h >= hmin)) status = 2;
+    if (status < 0) {
+      const double remaining = w.phase_len - w.t_phase;
+      const bool clamped = (double)w.h >= remaining;
+      const float h = clamped ? (float)remaining : w.h;
+      const bool joint = w.phase != kTransient;
+      w.steps++;
+      // state pass: every group computes it; the stage points become J coefficients
+      Jc jcs[7];
+      float x1[C], kx1[C], err_state = 0.f;
+      {
+        auto rhs = [&](int s, const float (&arg)[C], float (&out)[C]) {
+          rhs_state(arg, out, jcs[s], w.F, w.gam, left, right);
+        };
+        // stage 0 coefficients at the current state
+        float dummy[C];
+        rhs_state(w.x, dummy, jcs[0], w.F, w.gam, left, right);
+        dopri_pass(w.x, w.kx, h, rhs, x1, kx1, err_state, rtol, atol);
+      }
+      float err2 = (g == 0) ? err_state : 0.f;
+      if (joint) {
+        for (int r = 0; r < (k + G - 1) / G; r++) {
+          const int vec = r * G + g;
+          const bool valid = vec < k;
+          float v[C], kv[C], v1[C], kv1[C];
+#pragma unroll
+          for (int j = 0; j < C; j++) {
+            v[j] = valid ? V[vec * N + li * C + j] : 0.f;
+            kv[j] = valid ? KV[vec * N + li * C + j] : 0.f;
+          }
+          float e2 = 0.f;
+          auto rhs = [&](int s, const float (&arg)[C], float (&out)[C]) {
+            rhs_tangent(arg, out, jcs[s], w.gam, left, right);
+          };
+          dopri_pass(v, kv, h, rhs, v1, kv1, e2, rtol, atol);
+          if (valid) {
+            err2 += e2;
+#pragma unroll
+            for (int j = 0; j < C; j++) {
+              V1[vec * N + li * C + j] = v1[j];
+              KV1[vec * N + li * C + j] = kv1[j];
+            }
+          }
+        }
+      }
+      const float nc = joint ? (float)(N * (1 + k)) : (float)N;
+      const float err = sqrtf(warp_sum(err2) / nc);
+      if (!(err == err) || err > 3.0e38f) {
+        status = 1;
+      } else {
+        const float fac11 = exp2f(expo1 * __log2f(fmaxf(err, 1e-30f)));
+        if (err <= 1.0f) {
+          float fac = fac11 * exp2f(-beta * __log2f(w.fac_old));
+          fac = fmaxf(facc2, fminf(facc1, fac * (1.0f / safe)));
+          float hnew = h * __fdividef(1.0f, fac);
+          w.fac_old = fmaxf(err, 1e-4f);
+#pragma unroll
+          for (int j = 0; j < C; j++) {
+            w.x[j] = x1[j];
+            w.kx[j] = kx1[j];
+          }
+          __syncwarp();
+          if (joint) {  // accept the candidate: swap buffers
+            float *t0 = V, *t1 = KV;
+            V = V1;
+            KV = KV1;
+            V1 = t0;
+            KV1 = t1;
+            W = reinterpret_cast<double *>(V1 < KV1 ? V1 : KV1);
+          }
+          if ((double)hnew > hmax) hnew = (float)hmax;
+          if (w.reject && hnew > h) hnew = h;
+          w.reject = false;
+          if (!clamped || hnew < h) w.h = hnew;
+          w.t_phase = clamped ? w.phase_len : w.t_phase + (double)h;
+          w.t_gs += (double)h;
+          bool inside = true;
+#pragma unroll
+          for (int j = 0; j < C; j++) inside = inside && (fabsf(w.x[j]) <= esc);
+          if (!__all_sync(FULL, inside)) {
+            status = 4;
+          } else if (clamped) {
+            if (w.phase == kTransient) {
+              start_tangent();
+            } else if (w.phase == kAlign) {
+              if (!gram_schmidt()) status = 1;
+              w.phase = kAverage;
+              w.phase_len = w.t_avg;
+              w.t_phase = 0.0;
+            } else {
+              status = gram_schmidt() ? 0 : 1;
+            }
+          } else if (joint && w.t_gs >= w.L) {
+            if (!gram_schmidt()) status = 1;
+          }
+        } else {
+          w.h = h * __fdividef(1.0f, fminf(facc1, fac11 * (1.0f / safe)));
+          w.reject = true;
+        }
+      }
+    }
+    if (status >= 0) {
+      finish(w, a, k, lane, status);
+      w.pt = fetch(a, lane, a.P);
+      if (w.pt < a.P) start_point();
+    }
+  }
+}
+
+}  // namespace l96
+
+int launch_l96_warp(int integrator, int precision, const AdaptiveArgs &a, int, cudaStream_t s) {
+  using namespace l96;
+  if (integrator != kDopri5 || precision != kFP32) return kErrUnsupported;
+  if (a.k < 1 || a.k > N) return kErrUnsupported;
+  const size_t smem = (size_t)WARPS * 4 * a.k * N * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(l96_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return (int)e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned grid;
+  if (a.queue) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, l96_kernel, WARPS * 32, smem);
+    grid = (unsigned)std::min<int64_t>((int64_t)std::max(1, per_sm) * sms, (a.P + WARPS - 1) / WARPS);
+  } else {
+    grid = (unsigned)((a.P + WARPS - 1) / WARPS);
+  }
+  l96_kernel<<<grid, WARPS * 32, smem, s>>>(a);
+  return (int)cudaGetLastError();
+}
 
 }  // namespace chaos
