@@ -10,7 +10,8 @@ import importlib
 _EXPORTS = {
     "Sweep": "sweep", "SweepConfig": "sweep", "cuda_lyapunov": "sweep", "make_grid": "sweep",
     "make_inits": "sweep", "model_info": "sweep", "model_names": "sweep",
-    "fma_peak_tflops": "sweep", "ChaosError": "native", "LIB_PATH": "native",
+    "fma_peak_tflops": "sweep", "run_batch": "sweep", "BatchGraph": "sweep",
+    "ChaosError": "native", "LIB_PATH": "native",
 }
 
 __all__ = sorted(_EXPORTS)

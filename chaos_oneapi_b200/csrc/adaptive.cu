@@ -96,7 +96,119 @@ int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks,
   return kErrUnsupported;
 }
 
+// ----------------------------------------------------------- mixed batch
+// One persistent launch over segments of different models (3- and
+// 4-dimensional) and per-point averaging times.  A lane holds the state of
+// one point of one model at a time in a union sized for the largest model.
+// Points are handed out per segment: every lane starts in segment 0 and moves
+// to the next segment only when the current one is exhausted, so the lanes of
+// a warp run the same model (the same instruction stream) except briefly at
+// segment boundaries -- that is how points of uneven dimension and uneven
+// length are repacked without stranding warps.
+template <class R, int INTEG>
+union AnyLane {
+  Lane<Shimizu, 3, R, INTEG> shimizu;
+  Lane<Lorenz, 3, R, INTEG> lorenz;
+  Lane<Rossler, 3, R, INTEG> rossler;
+  Lane<Chua, 3, R, INTEG> chua;
+  Lane<HyperRossler, 4, R, INTEG> hyper;
+};
+
+template <class R, int INTEG, class Fn>
+__device__ __forceinline__ auto visit(int model, AnyLane<R, INTEG> &u, Fn &&fn) {
+  switch (model) {
+    case kShimizu: return fn(u.shimizu);
+    case kLorenz: return fn(u.lorenz);
+    case kRossler: return fn(u.rossler);
+    case kChua: return fn(u.chua);
+    default: return fn(u.hyper);
+  }
+}
+
+// Next point for this lane: from its current segment, or the following ones.
+__device__ __forceinline__ bool batch_next(const BatchArgs &b, int &seg, int64_t &pt) {
+  while (seg < b.nseg) {
+    const int64_t P = b.seg[seg].P;
+    const unsigned long long q = atomicAdd(&b.queues[seg], 1ULL);
+    if (q < (unsigned long long)P) {
+      pt = (int64_t)((q * (unsigned long long)b.seg[seg].queue_stride) % (unsigned long long)P);
+      return true;
+    }
+    ++seg;
+  }
+  return false;
+}
+
+template <class R, int INTEG>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 3 : 1) batch_kernel(const BatchArgs b) {
+  AnyLane<R, INTEG> u;
+  Ctl c{};
+  int seg = 0;
+  int64_t pt = 0;
+  bool active = batch_next(b, seg, pt);
+  auto start = [&]() {
+    c = make_ctl<R>(b.seg[seg]);
+    visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
+      lane_start(L, b.seg[seg], pt);
+      return 0;
+    });
+  };
+  if (active) start();
+  while (__any_sync(0xffffffffu, active)) {
+    if (active) {
+      const int r = visit<R, INTEG>(b.model[seg], u,
+                                    [&](auto &L) { return lane_step(L, b.seg[seg], c); });
+      if (r == kFinished) {
+        active = batch_next(b, seg, pt);
+        if (active) start();
+      }
+    }
+    const bool due = active && visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
+      return L.phase != kTransient && L.t_gs >= L.L;
+    });
+    if (__any_sync(0xffffffffu, due) && active) {
+      const bool failed = visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
+        if (L.phase == kTransient || !(L.t_gs > 0.0)) return false;
+        if (lane_gram_schmidt(L, b.seg[seg], c)) return false;
+        lane_finish(L, b.seg[seg], 1);
+        return true;
+      });
+      if (failed) {
+        active = batch_next(b, seg, pt);
+        if (active) start();
+      }
+    }
+  }
+}
+
 }  // namespace adaptive
+
+int launch_batch(int integ, int prec, const BatchArgs &b, int block, cudaStream_t s) {
+  using namespace adaptive;
+  if (b.nseg <= 0 || b.nseg > kMaxSegments) return kErrUnsupported;
+  int64_t total = 0;
+  for (int i = 0; i < b.nseg; i++) {
+    if (b.model[i] < 0 || b.model[i] >= kLorenz96) return kErrUnsupported;
+    const int dim = b.model[i] == kHyperRossler ? 4 : 3;
+    if (b.seg[i].k != dim) return kErrUnsupported;
+    total += b.seg[i].P;
+  }
+  if (total <= 0) return 0;
+  if (block <= 0 || block > 128 || block % 32) block = 128;
+  void (*kern)(BatchArgs) = nullptr;
+  if (integ == kDopri5 && prec == kFP32) kern = batch_kernel<float, kDopri5>;
+  else if (integ == kDopri5 && prec == kFP64) kern = batch_kernel<double, kDopri5>;
+  else if (integ == kDverk65 && prec == kFP32) kern = batch_kernel<float, kDverk65>;
+  else if (integ == kDverk65 && prec == kFP64) kern = batch_kernel<double, kDverk65>;
+  else return kErrUnsupported;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
+  const int64_t grid = std::min<int64_t>((int64_t)std::max(1, per_sm) * sms, (total + block - 1) / block);
+  kern<<<(unsigned)grid, block, 0, s>>>(b);
+  return (int)cudaGetLastError();
+}
 
 int launch_adaptive(int model, int integ, int prec, const AdaptiveArgs &a, int block,
                     int persistent_blocks, int variant, cudaStream_t s) {

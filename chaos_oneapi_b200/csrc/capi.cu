@@ -98,7 +98,7 @@ struct chaos_lyap_handle {
   int variant = 0;  // register-cap variant of the FP32 kernels (autotuned)
   cudaStream_t own_stream = nullptr;
   cudaStream_t last_stream = nullptr;
-  unsigned long long *queue = nullptr;  // persistent-schedule point counter
+  unsigned long long *queue = nullptr;  // point counters: persistent sweep / batch segments
   // host-path staging
   double *s_params = nullptr, *s_inits = nullptr, *s_spec = nullptr, *s_tavg = nullptr;
   int32_t *s_status = nullptr;
@@ -233,7 +233,7 @@ int chaos_lyap_create(const chaos_lyap_desc *desc, chaos_lyap_handle **out) {
     delete h;
     return cuda_fail(e, "cudaStreamCreate");
   }
-  if ((e = cudaMalloc(&h->queue, sizeof(unsigned long long))) != cudaSuccess) {
+  if ((e = cudaMalloc(&h->queue, sizeof(unsigned long long) * chaos::kMaxSegments)) != cudaSuccess) {
     cudaStreamDestroy(h->own_stream);
     delete h;
     return fail(CHAOS_LYAP_ENOMEM, "cudaMalloc(queue): %s", cudaGetErrorString(e));
@@ -464,6 +464,134 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   h->variant = best_v;
   if (block_out) *block_out = best_b;
   if (schedule_out) *schedule_out = best_s;
+  return CHAOS_LYAP_OK;
+}
+
+static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArgs *b,
+                       int *integ, int *prec, int *block) {
+  if (!segs || nseg <= 0 || nseg > chaos::kMaxSegments)
+    return fail(CHAOS_LYAP_EINVAL, "nseg must be 1..%d", chaos::kMaxSegments);
+  std::memset(b, 0, sizeof *b);
+  b->nseg = nseg;
+  for (int i = 0; i < nseg; i++) {
+    const chaos_lyap_segment &sg = segs[i];
+    if (!sg.handle) return fail(CHAOS_LYAP_EINVAL, "segment %d: null handle", i);
+    const chaos_lyap_desc &d = sg.handle->d;
+    if (d.precision == CHAOS_PREC_COMPAT_FP64 || sg.handle->model->dim > 4)
+      return fail(CHAOS_LYAP_EUNSUPPORTED,
+                  "segment %d: batches take the adaptive forms of 3-4 dimensional models", i);
+    if (i > 0 && (d.precision != segs[0].handle->d.precision ||
+                  d.integrator != segs[0].handle->d.integrator ||
+                  d.device != segs[0].handle->d.device))
+      return fail(CHAOS_LYAP_EINVAL, "segment %d: integrator / precision / device differ", i);
+    if (sg.P < 0 || (sg.P > 0 && (!sg.params || !sg.inits || !sg.spectrum)))
+      return fail(CHAOS_LYAP_EINVAL, "segment %d: bad arrays", i);
+    chaos::AdaptiveArgs &a = b->seg[i];
+    a.P = sg.P;
+    a.k = d.k;
+    a.gs = d.gs;
+    a.rtol = d.rtol;
+    a.atol = d.atol;
+    a.h0 = d.h;
+    a.hmax = d.h_max;
+    a.hmin = d.h_min;
+    a.t_transient = d.t_transient;
+    a.t_align = d.t_align;
+    a.t_avg = d.t_avg;
+    a.dt_renorm = d.dt_renorm;
+    a.max_steps = d.max_steps;
+    a.escape = d.escape > 0 ? d.escape : 1e4;
+    const ModelInfo *m = sg.handle->model;
+    a.params = cview(sg.params, sg.P, m->nparams, d.layout);
+    a.inits = cview(sg.inits, sg.P, m->dim, d.layout);
+    a.t_avg_per_point = sg.t_avg_per_point;
+    a.spectrum = view(sg.spectrum, sg.P, d.k, d.layout);
+    a.status = sg.status;
+    a.steps = sg.steps;
+    a.queue_stride = chaos::queue_stride_for(sg.P);
+    b->model[i] = m->id;
+  }
+  b->queues = segs[0].handle->queue;
+  const chaos_lyap_desc &d0 = segs[0].handle->d;
+  *integ = d0.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
+  *prec = d0.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
+  *block = segs[0].handle->block;
+  return CHAOS_LYAP_OK;
+}
+
+static int enqueue_batch(const chaos::BatchArgs &b, int integ, int prec, int block, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(b.queues, 0, sizeof(unsigned long long) * b.nseg, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
+  int rc = chaos::launch_batch(integ, prec, b, block, s);
+  if (rc == chaos::kErrUnsupported) return fail(CHAOS_LYAP_EUNSUPPORTED, "no batch kernel for this mix");
+  if (rc) return cuda_fail((cudaError_t)rc, "batch launch");
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream) {
+  chaos::BatchArgs b;
+  int integ, prec, block;
+  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block);
+  if (rc) return rc;
+  DeviceGuard g(segs[0].handle->d.device);
+  rc = enqueue_batch(b, integ, prec, block, (cudaStream_t)stream);
+  if (!rc) segs[0].handle->last_stream = (cudaStream_t)stream;
+  return rc;
+}
+
+struct chaos_lyap_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chaos_lyap_graph **out) {
+  if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
+  *out = nullptr;
+  chaos::BatchArgs b;
+  int integ, prec, block;
+  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block);
+  if (rc) return rc;
+  DeviceGuard g(segs[0].handle->d.device);
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  auto *gr = new chaos_lyap_graph();
+  gr->device = segs[0].handle->d.device;
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    rc = enqueue_batch(b, integ, prec, block, cs);
+    cudaError_t e2 = cudaStreamEndCapture(cs, &gr->graph);
+    if (!rc && e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
+  } else {
+    rc = cuda_fail(e, "cudaStreamBeginCapture");
+  }
+  if (!rc && (e = cudaGraphInstantiate(&gr->exec, gr->graph, 0)) != cudaSuccess)
+    rc = cuda_fail(e, "cudaGraphInstantiate");
+  cudaStreamDestroy(cs);
+  if (rc) {
+    if (gr->exec) cudaGraphExecDestroy(gr->exec);
+    if (gr->graph) cudaGraphDestroy(gr->graph);
+    delete gr;
+    return rc;
+  }
+  *out = gr;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_graph_launch(chaos_lyap_graph *g, void *stream) {
+  if (!g) return fail(CHAOS_LYAP_EINVAL, "graph is null");
+  DeviceGuard dg(g->device);
+  cudaError_t e = cudaGraphLaunch(g->exec, (cudaStream_t)stream);
+  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "cudaGraphLaunch");
+}
+
+int chaos_lyap_graph_destroy(chaos_lyap_graph *g) {
+  if (!g) return CHAOS_LYAP_OK;
+  DeviceGuard dg(g->device);
+  cudaGraphExecDestroy(g->exec);
+  cudaGraphDestroy(g->graph);
+  delete g;
   return CHAOS_LYAP_OK;
 }
 

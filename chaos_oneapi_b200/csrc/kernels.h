@@ -78,3 +78,20 @@ int launch_l96_warp(int integrator, int precision, const AdaptiveArgs &a, int wa
                     cudaStream_t s);
 
 }  // namespace chaos
+
+namespace chaos {
+
+// Mixed batch: up to kMaxSegments segments (each one model's points, with its
+// own arrays and phase times) swept by one persistent launch.  All segments
+// share the integrator and precision.
+constexpr int kMaxSegments = 8;
+struct BatchArgs {
+  int32_t nseg;
+  int32_t model[kMaxSegments];
+  AdaptiveArgs seg[kMaxSegments];  // seg[i].queue is not used; queue_stride is
+  unsigned long long *queues;      // nseg point counters, zeroed before the launch
+};
+
+int launch_batch(int integrator, int precision, const BatchArgs &b, int block, cudaStream_t s);
+
+}  // namespace chaos

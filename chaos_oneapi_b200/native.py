@@ -52,6 +52,13 @@ class Desc(ctypes.Structure):
     ]
 
 
+class Segment(ctypes.Structure):
+    _fields_ = [("handle", ctypes.c_void_p), ("P", ctypes.c_int64), ("params", ctypes.c_void_p),
+                ("inits", ctypes.c_void_p), ("spectrum", ctypes.c_void_p),
+                ("status", ctypes.c_void_p), ("steps", ctypes.c_void_p),
+                ("t_avg_per_point", ctypes.c_void_p)]
+
+
 class ChaosError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"chaos_lyap error {code}: {msg}")
@@ -81,6 +88,11 @@ SIGNATURES = {
     "chaos_lyap_autotune": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P,
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
+    "chaos_lyap_run_batch": (ctypes.c_int, [ctypes.POINTER(Segment), ctypes.c_int, _P]),
+    "chaos_lyap_batch_graph_create": (ctypes.c_int, [ctypes.POINTER(Segment), ctypes.c_int,
+                                                     ctypes.POINTER(_P)]),
+    "chaos_lyap_graph_launch": (ctypes.c_int, [_P, _P]),
+    "chaos_lyap_graph_destroy": (ctypes.c_int, [_P]),
     "chaos_lyap_get_variant": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
     "chaos_lyap_cudaLyapunov": (ctypes.c_int, [
         ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -236,3 +236,56 @@ def fma_peak_tflops(device: int = 0, precision: str = "fp32", seconds: float = 0
     out = ctypes.c_double()
     check(lib.chaos_lyap_fma_peak(device, native.PREC[precision], seconds, ctypes.byref(out)))
     return out.value
+
+
+def _segments(parts):
+    """parts: list of (Sweep, params, inits, spectrum, status, steps, t_avg) on CUDA."""
+    arr = (native.Segment * len(parts))()
+    for i, (sw, p, x, spec, st, steps, tavg) in enumerate(parts):
+        P = p.shape[0]
+        arr[i] = native.Segment(sw._h, P, _tptr(p, "float64").value, _tptr(x, "float64").value,
+                                _tptr(spec, "float64").value,
+                                None if st is None else _tptr(st, "int32").value,
+                                None if steps is None else _tptr(steps, "int64").value,
+                                None if tavg is None else _tptr(tavg, "float64").value)
+    return arr
+
+
+def run_batch(parts, stream=None):
+    """One launch over several sweeps (see chaos_lyap_run_batch)."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream().cuda_stream
+    elif hasattr(stream, "cuda_stream"):
+        stream = stream.cuda_stream
+    arr = _segments(parts)
+    check(lib.chaos_lyap_run_batch(arr, len(parts), ctypes.c_void_p(stream)))
+
+
+class BatchGraph:
+    """A mixed batch captured into a CUDA graph; replay with launch()."""
+
+    def __init__(self, parts):
+        self._parts = parts  # keep the tensors alive
+        self._g = ctypes.c_void_p()
+        check(lib.chaos_lyap_batch_graph_create(_segments(parts), len(parts),
+                                                ctypes.byref(self._g)))
+
+    def launch(self, stream=None):
+        import torch
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        check(lib.chaos_lyap_graph_launch(self._g, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self._g:
+            lib.chaos_lyap_graph_destroy(self._g)
+            self._g = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

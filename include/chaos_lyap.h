@@ -164,6 +164,35 @@ int chaos_lyap_sync(chaos_lyap_handle *h);
 int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
                         const double *inits, int32_t *block_out, int32_t *schedule_out);
 
+/* ---------------------------------------------------------- mixed batches
+ * Several sweeps (segments: different 3- or 4-dimensional models, each with
+ * its own handle, arrays and phase times; per-point averaging times allowed)
+ * in ONE persistent launch whose lanes take points segment after segment, so
+ * points of uneven dimension and length share warps without idling them.
+ * All handles must use the same integrator and precision; nseg <= 8.  The
+ * point counters live in the first segment's handle.  No reference
+ * counterpart (the reference launches one model per run, tasklyapunov.cpp:204). */
+typedef struct chaos_lyap_segment {
+  chaos_lyap_handle *handle;
+  int64_t P;
+  const double *params;
+  const double *inits;
+  double *spectrum;
+  int32_t *status;               /* optional */
+  int64_t *steps;                /* optional */
+  const double *t_avg_per_point; /* optional */
+} chaos_lyap_segment;
+
+int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream);
+
+/* The same batch captured once into a CUDA graph (counter reset + launch)
+ * and replayed by chaos_lyap_graph_launch on any stream; the segments'
+ * arrays are baked in: refill them and replay. */
+typedef struct chaos_lyap_graph chaos_lyap_graph;
+int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chaos_lyap_graph **out);
+int chaos_lyap_graph_launch(chaos_lyap_graph *g, void *stream);
+int chaos_lyap_graph_destroy(chaos_lyap_graph *g);
+
 /* The FP32 kernel variant in use (desc.variant, or the autotuner's choice). */
 int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);
 
