@@ -38,6 +38,7 @@ CUDA_UNITS = {
     "l96.cu": [],
     "capi.cu": [],
     "peak.cu": [],
+    "static_scratch.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]
 HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp",

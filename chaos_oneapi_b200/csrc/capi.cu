@@ -89,6 +89,16 @@ chaos::CView cview(const double *p, int64_t P, int C, int layout) {
 
 }  // namespace
 
+namespace chaos {
+int model_id_of(const char *name, int *dim, int *nparams) {
+  const ModelInfo *m = find_model(name);
+  if (!m) return -1;
+  if (dim) *dim = m->dim;
+  if (nparams) *nparams = m->nparams;
+  return m->id;
+}
+}  // namespace chaos
+
 struct chaos_lyap_handle {
   chaos_lyap_desc d;
   const ModelInfo *model;

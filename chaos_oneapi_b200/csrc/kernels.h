@@ -95,3 +95,9 @@ struct BatchArgs {
 int launch_batch(int integrator, int precision, const BatchArgs &b, int block, cudaStream_t s);
 
 }  // namespace chaos
+
+namespace chaos {
+// Registry lookup shared by the C ABI translation units: model id, dimension
+// and parameter count of a registered name; -1 when unknown.
+int model_id_of(const char *name, int *dim, int *nparams);
+}  // namespace chaos

@@ -193,6 +193,23 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
 int chaos_lyap_graph_launch(chaos_lyap_graph *g, void *stream);
 int chaos_lyap_graph_destroy(chaos_lyap_graph *g);
 
+/* The mixed batch above for callers that cannot allocate device memory while
+ * they run: their device memory belongs to their own allocator, or an
+ * allocation (and the synchronisation a free implies) would stall a real-time
+ * loop, or their plugin host forbids device allocations.  No counterpart in
+ * the reference.  Takes one descriptor per segment instead of handles
+ * (segs[i].handle is ignored) and allocates nothing: the batch kernel's point
+ * counters live in a fixed 8-entry device array inside the library, which
+ * every GPU that loads it holds until the process exits, so nseg > 8 is
+ * rejected.  All calls share those counters: calls that overlap on the GPU
+ * race, so serialise them.  Each call zeroes the counters it uses on `stream`
+ * before launching.  The first call on a device looks up the array's device
+ * address; make it before any stream capture begins.  On failure the message
+ * is in chaos_lyap_static_last_error(). */
+int chaos_lyap_run_batch_static(const chaos_lyap_desc *descs, const chaos_lyap_segment *segs,
+                                int nseg, void *stream);
+const char *chaos_lyap_static_last_error(void);
+
 /* The FP32 kernel variant in use (desc.variant, or the autotuner's choice). */
 int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);
 
