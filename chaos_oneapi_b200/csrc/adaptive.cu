@@ -100,11 +100,15 @@ int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks,
 // One persistent launch over segments of different models (3- and
 // 4-dimensional) and per-point averaging times.  A lane holds the state of
 // one point of one model at a time in a union sized for the largest model.
-// Points are handed out per segment: every lane starts in segment 0 and moves
-// to the next segment only when the current one is exhausted, so the lanes of
-// a warp run the same model (the same instruction stream) except briefly at
-// segment boundaries -- that is how points of uneven dimension and uneven
-// length are repacked without stranding warps.
+// Every warp works on one segment at a time (warps start on segments round
+// robin), and a lane that finishes a point takes the next point of its warp's
+// segment: within a segment, lanes refill independently, so uneven point
+// lengths do not strand warps, and since all lanes of a warp run the same
+// model they share one instruction stream.  When its segment has no points
+// left, a lane idles until the whole warp is idle; the warp then moves to the
+// next segment that still has points.  (Letting lanes move on individually
+// mixes models inside warps, which runs every model's step code for the warp
+// and measured slower than three separate launches.)
 template <class R, int INTEG>
 union AnyLane {
   Lane<Shimizu, 3, R, INTEG> shimizu;
@@ -125,56 +129,62 @@ __device__ __forceinline__ auto visit(int model, AnyLane<R, INTEG> &u, Fn &&fn) 
   }
 }
 
-// Next point for this lane: from its current segment, or the following ones.
-__device__ __forceinline__ bool batch_next(const BatchArgs &b, int &seg, int64_t &pt) {
-  while (seg < b.nseg) {
-    const int64_t P = b.seg[seg].P;
-    const unsigned long long q = atomicAdd(&b.queues[seg], 1ULL);
-    if (q < (unsigned long long)P) {
-      pt = (int64_t)((q * (unsigned long long)b.seg[seg].queue_stride) % (unsigned long long)P);
-      return true;
-    }
-    ++seg;
-  }
-  return false;
+// Next point of segment `seg` for this lane, if any is left.
+__device__ __forceinline__ bool batch_take(const BatchArgs &b, int seg, int64_t &pt) {
+  const int64_t P = b.seg[seg].P;
+  const unsigned long long q = atomicAdd(&b.queues[seg], 1ULL);
+  if (q >= (unsigned long long)P) return false;
+  pt = (int64_t)((q * (unsigned long long)b.seg[seg].queue_stride) % (unsigned long long)P);
+  return true;
 }
 
 template <class R, int INTEG>
 __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 3 : 1) batch_kernel(const BatchArgs b) {
   AnyLane<R, INTEG> u;
   Ctl c{};
-  int seg = 0;
+  const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  int wseg = warp % b.nseg;  // the warp's segment (warp-uniform)
+  int tried = 0;             // segments found empty since the warp last got work
   int64_t pt = 0;
-  bool active = batch_next(b, seg, pt);
   auto start = [&]() {
-    c = make_ctl<R>(b.seg[seg]);
-    visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
-      lane_start(L, b.seg[seg], pt);
+    c = make_ctl<R>(b.seg[wseg]);
+    visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
+      lane_start(L, b.seg[wseg], pt);
       return 0;
     });
   };
+  bool active = batch_take(b, wseg, pt);
   if (active) start();
-  while (__any_sync(0xffffffffu, active)) {
+  for (;;) {
+    if (!__any_sync(0xffffffffu, active)) {
+      // the whole warp is idle: next segment with points left, or done
+      if (++tried >= b.nseg) break;
+      wseg = (wseg + 1) % b.nseg;
+      active = batch_take(b, wseg, pt);
+      if (active) start();
+      continue;
+    }
+    tried = 0;
     if (active) {
-      const int r = visit<R, INTEG>(b.model[seg], u,
-                                    [&](auto &L) { return lane_step(L, b.seg[seg], c); });
+      const int r = visit<R, INTEG>(b.model[wseg], u,
+                                    [&](auto &L) { return lane_step(L, b.seg[wseg], c); });
       if (r == kFinished) {
-        active = batch_next(b, seg, pt);
+        active = batch_take(b, wseg, pt);
         if (active) start();
       }
     }
-    const bool due = active && visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
+    const bool due = active && visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
       return L.phase != kTransient && L.t_gs >= L.L;
     });
     if (__any_sync(0xffffffffu, due) && active) {
-      const bool failed = visit<R, INTEG>(b.model[seg], u, [&](auto &L) {
+      const bool failed = visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
         if (L.phase == kTransient || !(L.t_gs > 0.0)) return false;
-        if (lane_gram_schmidt(L, b.seg[seg], c)) return false;
-        lane_finish(L, b.seg[seg], 1);
+        if (lane_gram_schmidt(L, b.seg[wseg], c)) return false;
+        lane_finish(L, b.seg[wseg], 1);
         return true;
       });
       if (failed) {
-        active = batch_next(b, seg, pt);
+        active = batch_take(b, wseg, pt);
         if (active) start();
       }
     }
