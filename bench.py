@@ -221,6 +221,67 @@ BATCH_KW = dict(method="var", integrator="dopri5", precision="fp32", rtol=1e-6, 
                 h=1e-2, t_transient=100.0, t_avg=5500.0, dt_renorm=1.0)
 
 
+def run_surrogate_bench(a, rank, world, local):
+    """--workload surrogate: a Lorenz (sigma, rho) map of --map-size^2 cells
+    (sigma in [5, 20], rho in [0, 200]) refined by the MLP ensemble, against
+    the plain FP64 sweep (DVERK 6(5) rtol 1e-10, transient 100, averaging
+    1000), whose full-map time is extrapolated from a timed random sample of
+    2^18 cells; regime agreement on 10,000 seeded held-out cells."""
+    import torch
+    import chaos_oneapi_b200 as cl
+    from chaos_oneapi_b200.surrogate import MapSpec, RefineConfig, plain_sweep, refine_map
+    torch.cuda.set_device(local)
+    n = a.map_size
+    spec = MapSpec("lorenz", [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, n], [1, 0.0, 200.0, n],
+                   [1.0, 1.0, 1.0], seed=rank)
+    sw = cl.Sweep(model="lorenz", method="var", integrator="dverk65", precision="fp64",
+                  rtol=1e-10, atol=1e-10, h=1e-3, t_transient=100.0, t_avg=1000.0, dt_renorm=1.0,
+                  device=local)
+    P = n * n
+    rng = np.random.default_rng(2024)
+    held = rng.choice(P, 10000, replace=False)
+    truth, st = plain_sweep(sw, spec, held)
+    sample = rng.choice(P, min(P, 1 << 18), replace=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_sweep(sw, spec, sample)
+    plain_est = (time.perf_counter() - t0) * P / sample.size
+    cfg = RefineConfig(steps0=6000, steps_round=4000, rounds=4, round_grid_step=max(1, n // 512),
+                       round_max_new=65536)
+    clocks = ClockSampler(local)
+    clocks.start()
+    out, mask, info = refine_map(spec, sw, cfg)
+    clk = clocks.stop()
+    refined = info["timings"]["total_s"]
+    ok = st == 0
+    agree = float(((out[held, 0] > 0.01) == (truth[:, 0] > 0.01))[ok].mean())
+    d = np.abs(out[held] - truth)[ok]
+    filled = ~mask[held][ok]
+    if rank == 0:
+        line = {
+            "metric": METRIC + " (surrogate-refined map)", "value": P / refined, "unit": "points/s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * refined,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64+bf16",
+            "data": "synthetic (seeded grid and jitter)",
+            "config": {"workload": "surrogate", "map": f"{n}x{n} Lorenz (sigma, rho)",
+                       "plain": "DVERK 6(5) FP64 rtol 1e-10, T 100 + 1000, renorm 1",
+                       "ensemble": "4 x MLP 16 Fourier features -> 128 -> 128 -> 128 -> 3, "
+                                   "SiLU, BF16 mma.sync, FP32 accumulate, Adam 1e-3",
+                       "rule": "integrate where std(lambda_1) > 0.02 or |lambda_1| < 0.05",
+                       "rounds": cfg.rounds, "round_max_new": cfg.round_max_new},
+            "refined_s": refined, "plain_estimate_s": plain_est,
+            "refined_over_plain": refined / plain_est,
+            "plain_fraction": info["plain_fraction"], "training_cells": info["training_cells"],
+            "timings": info["timings"], "clocks": clk,
+            "held_out": {"cells": int(ok.sum()), "regime_agreement": agree,
+                         "surrogate_filled": int(filled.sum()),
+                         "median_abs_err_filled": ([float(x) for x in np.median(d[filled], 0)]
+                                                   if filled.any() else None)},
+            "gpu_launches": None,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_batch_bench(a, rank, world, local):
     """--workload batch256: the mixed batch through a CUDA graph, beside the
     same three sweeps launched one after another without the work queue."""
@@ -350,7 +411,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rossler1024", choices=sorted(WORKLOADS) + ["batch256"])
+    ap.add_argument("--workload", default="rossler1024",
+                    choices=sorted(WORKLOADS) + ["batch256", "surrogate"])
+    ap.add_argument("--map-size", type=int, default=4096, help="surrogate workload: cells per side")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-sample", type=int, default=256)
     ap.add_argument("--variant", type=int, default=-1,
@@ -363,6 +426,15 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     a.gpus = max(a.gpus, world)
 
+    if a.workload == "surrogate":
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no surrogate form"}))
+            return
+        if rank == 0:
+            run_surrogate_bench(a, rank, world, local)
+        return
     if a.workload == "batch256":
         if a.impl == "reference":
             if rank == 0:

@@ -39,6 +39,7 @@ CUDA_UNITS = {
     "capi.cu": [],
     "peak.cu": [],
     "static_scratch.cu": [],
+    "mlp.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]
 HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp",
@@ -71,7 +72,7 @@ def _deps_mtime(dirs) -> float:
         for f in os.listdir(d):
             if f.endswith((".h", ".cuh", ".hpp")):
                 t = max(t, os.path.getmtime(os.path.join(d, f)))
-    for h in ("chaos_lyap.h", "chaos_lyap_host.h"):
+    for h in ("chaos_lyap.h", "chaos_lyap_host.h", "chaos_lyap_surrogate.h"):
         t = max(t, os.path.getmtime(os.path.join(ROOT, "include", h)))
     return t
 

@@ -5,6 +5,7 @@
 // independent samples).
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/chaos_lyap.h"
 
@@ -87,6 +88,36 @@ int chaos_lyap_make_inits(int32_t n, int64_t P, const double *base, double amp, 
         out[p * n + blk * 4 + q] = base[blk * 4 + q] + d;
       }
     }
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_make_inits_at(int32_t n, int64_t count, const int64_t *index, const double *base,
+                             double amp, int32_t dist, uint64_t seed, double *out) {
+  if (n <= 0 || count < 0 || !index || !base || !out || (dist != 0 && dist != 1))
+    return CHAOS_LYAP_EINVAL;
+  std::vector<double> one(n);
+  for (int64_t i = 0; i < count; ++i) {
+    // the point's own counter block, as chaos_lyap_make_inits would draw it
+    const int64_t p = index[i];
+    const uint64_t key[2] = {seed, 0x6368616F735F6C79ULL};
+    for (int blk = 0; blk * 4 < n; ++blk) {
+      const uint64_t ctr[4] = {(uint64_t)p, (uint64_t)blk, 0, 0};
+      uint64_t r[4];
+      philox4x64(ctr, key, r);
+      for (int q = 0; q < 4 && blk * 4 + q < n; ++q) {
+        double d;
+        if (dist == 0) {
+          d = (2.0 * unit53(r[q]) - 1.0) * amp;
+        } else {
+          const double u1 = 1.0 - unit53(r[q & ~1]), u2 = unit53(r[q | 1]);
+          const double rad = std::sqrt(-2.0 * std::log(u1));
+          const double ang = 6.283185307179586 * u2;
+          d = amp * ((q & 1) ? rad * std::sin(ang) : rad * std::cos(ang));
+        }
+        out[i * n + blk * 4 + q] = base[blk * 4 + q] + d;
+      }
+    }
+  }
   return CHAOS_LYAP_OK;
 }
 

@@ -1,0 +1,690 @@
+// Learned surrogate: an ensemble of small MLPs mapping a parameter point
+// (p1, p2) to its Lyapunov spectrum, trained and evaluated on the GPU by the
+// kernels below (no library GEMM).
+//
+//   features: 16 Fourier features of the point normalised to [0, 1]^2:
+//             sin / cos (2 pi w_f . (u, v)) for 8 frequency vectors (default
+//             sin / cos (pi j u), sin / cos (pi j v), j = 1..4)
+//   network:  16 -> W -> W -> W -> 3 (W = 128), SiLU between layers
+//   numerics: weights and activations in BF16 for the tensor-core products
+//             (mma.sync m16n8k16, FP32 accumulate); FP32 master weights, FP32
+//             pre-activations for the backward pass, FP32 Adam moments
+//
+// All E networks advance together: every kernel takes the network index from
+// blockIdx.z.  The loss is the mean squared error of standardised targets
+// (each exponent shifted and scaled by the training data's mean and std).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/chaos_lyap.h"
+#include "../../include/chaos_lyap_surrogate.h"
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kFeat = 16;   // input features
+constexpr int kOutPad = 16; // output width padded for the tensor-core tiles
+
+thread_local std::string g_err;
+int fail(int code, const std::string &m) {
+  g_err = m;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+  return fail(CHAOS_LYAP_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------- GEMM
+// C[z](m, n) = sum_k A[z](m, k) B[z](k, n), A and B in BF16 at arbitrary
+// strides, C in FP32 (row-major, ldc).  64 x 64 tile per block, 4 warps of
+// 32 x 32, k in steps of 16 staged through shared memory so that the
+// fragments of mma.sync.m16n8k16 are contiguous pairs.
+struct GemmArgs {
+  int M, N, K;
+  const bf16 *A;
+  int64_t sam, sak, saz;  // A(m, k) = A[z * saz + m * sam + k * sak]
+  const bf16 *B;
+  int64_t sbk, sbn, sbz;  // B(k, n) = B[z * sbz + k * sbk + n * sbn]
+  float *C;
+  int64_t ldc, scz;
+  int accumulate;         // 1: C += A B
+};
+
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
+  __shared__ __align__(16) bf16 As[64][16 + 8];  // [m][k], padded rows
+  __shared__ __align__(16) bf16 Bs[64][16 + 8];  // [n][k]
+  const int z = blockIdx.z;
+  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int grp = lane >> 2, tig = lane & 3;
+  const bf16 *A = g.A + z * g.saz;
+  const bf16 *B = g.B + z * g.sbz;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
+  const bf16 zero = __float2bfloat16(0.f);
+  for (int k0 = 0; k0 < g.K; k0 += 16) {
+    // stage 64 x 16 of A and 16 x 64 of B (8 elements per thread each)
+    for (int e = tid; e < 64 * 16; e += 128) {
+      const int r = e >> 4, kk = e & 15;
+      const int m = m0 + r, k = k0 + kk;
+      As[r][kk] = (m < g.M && k < g.K) ? A[m * g.sam + k * g.sak] : zero;
+      const int n = n0 + r;
+      Bs[r][kk] = (n < g.N && k < g.K) ? B[k * g.sbk + n * g.sbn] : zero;
+    }
+    __syncthreads();
+    uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+      const int r = wm + i * 16 + grp;
+      af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][tig * 2]);
+      af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][tig * 2]);
+      af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][tig * 2 + 8]);
+      af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][tig * 2 + 8]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int c = wn + j * 8 + grp;
+      bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][tig * 2]);
+      bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][tig * 2 + 8]);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+            "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
+            : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]),
+              "r"(bfr[j][1]));
+      }
+    __syncthreads();
+  }
+  float *C = g.C + z * g.scz;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const int m = m0 + wm + i * 16 + grp + (r >= 2 ? 8 : 0);
+        const int n = n0 + wn + j * 8 + tig * 2 + (r & 1);
+        if (m < g.M && n < g.N) {
+          float *p = &C[m * g.ldc + n];
+          *p = g.accumulate ? *p + acc[i][j][r] : acc[i][j][r];
+        }
+      }
+}
+
+int gemm(const GemmArgs &g, int nz, cudaStream_t s) {
+  dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, nz);
+  gemm_bf16_kernel<<<grid, 128, 0, s>>>(g);
+  return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------- elementwise parts
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float sg = 1.f / (1.f + __expf(-z));
+  return sg * (1.f + z * (1.f - sg));
+}
+
+// 16 Fourier features of the normalised point (shared by all networks):
+// sin and cos of 2 pi (w_f . (u, v)) for 8 frequency vectors w_f.
+struct Freqs {
+  float w[8][2];
+};
+__global__ void features_kernel(const double *xy, int64_t N, double u0, double us, double v0,
+                                double vs, Freqs fr, bf16 *X) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const float u = (float)((xy[2 * i] - u0) * us), v = (float)((xy[2 * i + 1] - v0) * vs);
+#pragma unroll
+  for (int f = 0; f < 8; f++) {
+    float sn, cs;
+    sincospif(2.f * (fr.w[f][0] * u + fr.w[f][1] * v), &sn, &cs);
+    X[i * kFeat + 2 * f] = __float2bfloat16(sn);
+    X[i * kFeat + 2 * f + 1] = __float2bfloat16(cs);
+  }
+}
+
+// Z += b (per column); A = SiLU(Z) in BF16.  z = network.
+__global__ void bias_silu_kernel(float *Z, const float *b, int64_t sbz, bf16 *A, int64_t rows,
+                                 int cols, int64_t sz) {
+  const int z = blockIdx.z;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  const int c = (int)(i % cols);
+  const float v = Z[z * sz + i] + b[z * sbz + c];
+  Z[z * sz + i] = v;
+  A[z * sz + i] = __float2bfloat16(silu(v));
+}
+
+// Output layer: Y = Z + b on the first `outs` columns; for training, the
+// loss gradient dY = 2 (Y - T) / (rows * outs) in BF16 (zero on the padding)
+// and the squared error summed into loss[z].
+__global__ void output_kernel(float *Y, const float *b, int64_t sbz, int64_t rows, int outs,
+                              const float *T, const float *tmean, const float *tinv, bf16 *dY,
+                              float *loss) {
+  const int z = blockIdx.z;
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  float l = 0.f;
+  for (int c = 0; c < kOutPad; c++) {
+    float *y = &Y[(z * rows + r) * kOutPad + c];
+    if (c < outs) {
+      *y += b[z * sbz + c];
+      if (T) {
+        const float t = (T[r * outs + c] - tmean[c]) * tinv[c];
+        const float d = *y - t;
+        l += d * d;
+        dY[(z * rows + r) * kOutPad + c] = __float2bfloat16(2.f * d / (float)(rows * outs));
+      }
+    } else if (T) {
+      dY[(z * rows + r) * kOutPad + c] = __float2bfloat16(0.f);
+    }
+  }
+  if (T) atomicAdd(&loss[z], l / (float)(rows * outs));
+}
+
+// dZ = dA * SiLU'(Z) in BF16 (dA in FP32, from the transposed product).
+__global__ void silu_back_kernel(const float *dA, const float *Z, bf16 *dZ, int64_t n, int64_t sz) {
+  const int z = blockIdx.z;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dZ[z * sz + i] = __float2bfloat16(dA[z * sz + i] * dsilu(Z[z * sz + i]));
+}
+
+// db[c] = sum_r dZ[r, c] (one thread per column, per network).
+__global__ void bias_grad_kernel(const bf16 *dZ, int64_t rows, int cols, int64_t sz, float *db,
+                                 int64_t sdz) {
+  const int z = blockIdx.z;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.f;
+  for (int64_t r = 0; r < rows; r++) s += __bfloat162float(dZ[z * sz + r * cols + c]);
+  db[z * sdz + c] = s;
+}
+
+// Adam on the FP32 master parameters, then the BF16 copy of the weights.
+__global__ void adam_kernel(float *p, const float *gr, float *m, float *v, bf16 *pb, int64_t n,
+                            float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float g = gr[i];
+  const float mi = b1 * m[i] + (1.f - b1) * g;
+  const float vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float upd = lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  p[i] -= upd;
+  pb[i] = __float2bfloat16(p[i]);
+}
+
+__global__ void to_bf16_kernel(const float *p, bf16 *pb, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pb[i] = __float2bfloat16(p[i]);
+}
+
+// Ensemble mean and standard deviation (de-standardised) of the outputs.
+__global__ void ensemble_kernel(const float *Y, int E, int64_t rows, int outs, const float *tmean,
+                                const float *tstd, float *mean, float *std) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  for (int c = 0; c < outs; c++) {
+    float s = 0.f, s2 = 0.f;
+    for (int z = 0; z < E; z++) {
+      const float y = Y[(z * rows + r) * kOutPad + c] * tstd[c] + tmean[c];
+      s += y;
+      s2 += y * y;
+    }
+    const float mu = s / E;
+    if (mean) mean[r * outs + c] = mu;
+    if (std) std[r * outs + c] = sqrtf(fmaxf(s2 / E - mu * mu, 0.f));
+  }
+}
+
+inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// Parameter layout per network (FP32 master, BF16 copy, Adam moments):
+//   W1 [16 x W] b1 [W] W2 [W x W] b2 [W] W3 [W x W] b3 [W] W4 [W x 16] b4 [16]
+// (W4 and b4 padded to 16 outputs; the padding stays zero).
+struct chaos_mlp {
+  int E, W, outs, device;
+  int64_t np;  // parameters per network
+  int64_t off_w[4], off_b[4];
+  float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
+  bf16 *pb = nullptr;
+  float tmean[kOutPad], tstd[kOutPad];
+  float *d_tmean = nullptr, *d_tstd = nullptr, *d_tinv = nullptr;
+  double u0 = 0, us = 1, v0 = 0, vs = 1;
+  Freqs freqs;    // feature frequencies (cycles over the unit box)
+  int64_t t = 0;  // Adam step
+  // workspace for `cap` rows
+  int64_t cap = 0;
+  bf16 *X = nullptr, *A1 = nullptr, *A2 = nullptr, *A3 = nullptr, *dZ = nullptr, *dY = nullptr;
+  float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *Y = nullptr, *dA = nullptr, *loss = nullptr;
+  float *Tb = nullptr;
+  double *xyb = nullptr;
+};
+
+namespace {
+
+void free_ws(chaos_mlp *h) {
+  void *ps[] = {h->X, h->A1, h->A2, h->A3, h->dZ, h->dY, h->Z1, h->Z2, h->Z3, h->Y, h->dA, h->Tb,
+                h->xyb};
+  for (void *p : ps) cudaFree(p);
+  h->X = h->A1 = h->A2 = h->A3 = h->dZ = h->dY = nullptr;
+  h->Z1 = h->Z2 = h->Z3 = h->Y = h->dA = h->Tb = nullptr;
+  h->xyb = nullptr;
+  h->cap = 0;
+}
+
+int ensure_ws(chaos_mlp *h, int64_t rows) {
+  if (rows <= h->cap) return 0;
+  free_ws(h);
+  const int64_t E = h->E, W = h->W;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](void **p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  al((void **)&h->X, sizeof(bf16) * rows * kFeat);
+  al((void **)&h->A1, sizeof(bf16) * E * rows * W);
+  al((void **)&h->A2, sizeof(bf16) * E * rows * W);
+  al((void **)&h->A3, sizeof(bf16) * E * rows * W);
+  al((void **)&h->dZ, sizeof(bf16) * E * rows * W);
+  al((void **)&h->dY, sizeof(bf16) * E * rows * kOutPad);
+  al((void **)&h->Z1, sizeof(float) * E * rows * W);
+  al((void **)&h->Z2, sizeof(float) * E * rows * W);
+  al((void **)&h->Z3, sizeof(float) * E * rows * W);
+  al((void **)&h->Y, sizeof(float) * E * rows * kOutPad);
+  al((void **)&h->dA, sizeof(float) * E * rows * W);
+  al((void **)&h->Tb, sizeof(float) * rows * kOutPad);
+  al((void **)&h->xyb, sizeof(double) * rows * 2);
+  if (e != cudaSuccess) {
+    free_ws(h);
+    return fail(CHAOS_LYAP_ENOMEM, std::string("surrogate workspace: ") + cudaGetErrorString(e));
+  }
+  h->cap = rows;
+  return 0;
+}
+
+GemmArgs mk(int M, int N, int K, const bf16 *A, int64_t sam, int64_t sak, int64_t saz, const bf16 *B,
+            int64_t sbk, int64_t sbn, int64_t sbz, float *C, int64_t ldc, int64_t scz, int acc = 0) {
+  return GemmArgs{M, N, K, A, sam, sak, saz, B, sbk, sbn, sbz, C, ldc, scz, acc};
+}
+
+// Forward pass of all networks on `rows` points (features already in h->X).
+int forward(chaos_mlp *h, int64_t rows, cudaStream_t s) {
+  const int E = h->E, W = h->W;
+  const int64_t np = h->np, sz = rows * W;
+  const bf16 *Wb = h->pb;
+  int rc = 0;
+  // Z1 = X W1 ; A1 = silu(Z1 + b1)
+  rc |= gemm(mk(rows, W, kFeat, h->X, kFeat, 1, 0, Wb + h->off_w[0], W, 1, np, h->Z1, W, sz), E, s);
+  bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z1, h->p + h->off_b[0], np, h->A1, rows, W, sz);
+  rc |= gemm(mk(rows, W, W, h->A1, W, 1, sz, Wb + h->off_w[1], W, 1, np, h->Z2, W, sz), E, s);
+  bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z2, h->p + h->off_b[1], np, h->A2, rows, W, sz);
+  rc |= gemm(mk(rows, W, W, h->A2, W, 1, sz, Wb + h->off_w[2], W, 1, np, h->Z3, W, sz), E, s);
+  bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z3, h->p + h->off_b[2], np, h->A3, rows, W, sz);
+  rc |= gemm(mk(rows, kOutPad, W, h->A3, W, 1, sz, Wb + h->off_w[3], kOutPad, 1, np, h->Y, kOutPad,
+                rows * kOutPad), E, s);
+  if (rc) return rc;
+  return (int)cudaGetLastError();
+}
+
+// Backward pass after forward + output_kernel (dY set); gradients into h->g.
+int backward(chaos_mlp *h, int64_t rows, cudaStream_t s) {
+  const int E = h->E, W = h->W;
+  const int64_t np = h->np, sz = rows * W, syz = rows * kOutPad;
+  const bf16 *Wb = h->pb;
+  float *g = h->g;
+  int rc = 0;
+  // layer 4: dW4 = A3^T dY ; db4 = sum dY ; dA3 = dY W4^T
+  rc |= gemm(mk(W, kOutPad, rows, h->A3, 1, W, sz, h->dY, kOutPad, 1, syz, g + h->off_w[3], kOutPad, np), E, s);
+  bias_grad_kernel<<<dim3(1, 1, E), kOutPad, 0, s>>>(h->dY, rows, kOutPad, syz, g + h->off_b[3], np);
+  rc |= gemm(mk(rows, W, kOutPad, h->dY, kOutPad, 1, syz, Wb + h->off_w[3], 1, kOutPad, np, h->dA, W, sz), E, s);
+  // layer 3
+  silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z3, h->dZ, sz, sz);
+  rc |= gemm(mk(W, W, rows, h->A2, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[2], W, np), E, s);
+  bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[2], np);
+  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[2], 1, W, np, h->dA, W, sz), E, s);
+  // layer 2
+  silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z2, h->dZ, sz, sz);
+  rc |= gemm(mk(W, W, rows, h->A1, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[1], W, np), E, s);
+  bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[1], np);
+  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[1], 1, W, np, h->dA, W, sz), E, s);
+  // layer 1
+  silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z1, h->dZ, sz, sz);
+  rc |= gemm(mk(kFeat, W, rows, h->X, 1, kFeat, 0, h->dZ, W, 1, sz, g + h->off_w[0], W, np), E, s);
+  bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[0], np);
+  if (rc) return rc;
+  return (int)cudaGetLastError();
+}
+
+// One forward / backward on `rows` points starting at xy / T (device).
+int grad_step(chaos_mlp *h, const double *xy, const float *T, int64_t rows, cudaStream_t s) {
+  features_kernel<<<blocks(rows, 256), 256, 0, s>>>(xy, rows, h->u0, h->us, h->v0, h->vs, h->freqs,
+                                                    h->X);
+  int rc = forward(h, rows, s);
+  if (rc) return rc;
+  cudaMemsetAsync(h->loss, 0, sizeof(float) * h->E, s);
+  output_kernel<<<dim3(blocks(rows, 128), 1, h->E), 128, 0, s>>>(
+      h->Y, h->p + h->off_b[3], h->np, rows, h->outs, T, h->d_tmean, h->d_tinv, h->dY, h->loss);
+  return backward(h, rows, s);
+}
+
+// Deterministic uniform(-1, 1) for the initial weights.
+inline float uhash(uint64_t seed, uint64_t i) {
+  uint64_t x = seed * 0x9E3779B97F4A7C15ULL + i * 0xBF58476D1CE4E5B9ULL + 0x94D049BB133111EBULL;
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ULL;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBULL;
+  x ^= x >> 31;
+  return (float)((x >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
+}
+
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DevGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char *chaos_mlp_last_error(void) { return g_err.c_str(); }
+
+int chaos_mlp_create(int ensemble, int width, int outputs, uint64_t seed, int device,
+                     chaos_mlp **out) {
+  if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
+  *out = nullptr;
+  if (ensemble < 1 || ensemble > 16 || width < 16 || width > 1024 || width % 16 ||
+      outputs < 1 || outputs > kOutPad)
+    return fail(CHAOS_LYAP_EINVAL, "ensemble 1..16, width multiple of 16 in 16..1024, outputs 1..16");
+  DevGuard g(device);
+  auto *h = new chaos_mlp();
+  h->E = ensemble;
+  h->W = width;
+  h->outs = outputs;
+  h->device = device;
+  const int64_t W = width;
+  const int64_t sizes_w[4] = {kFeat * W, W * W, W * W, W * kOutPad};
+  const int64_t sizes_b[4] = {W, W, W, kOutPad};
+  int64_t off = 0;
+  for (int l = 0; l < 4; l++) {
+    h->off_w[l] = off;
+    off += sizes_w[l];
+    h->off_b[l] = off;
+    off += sizes_b[l];
+  }
+  h->np = off;
+  const int64_t n = h->np * ensemble;
+  // He-style uniform init, scaled by fan-in; zero biases and output padding
+  std::vector<float> init(n, 0.f);
+  const int64_t fan_in[4] = {kFeat, W, W, W};
+  const int64_t cols[4] = {W, W, W, kOutPad};
+  for (int z = 0; z < ensemble; z++)
+    for (int l = 0; l < 4; l++) {
+      const float a = std::sqrt(6.f / (float)fan_in[l]) * (l == 3 ? 0.5f : 1.f);
+      for (int64_t i = 0; i < sizes_w[l]; i++) {
+        const int64_t col = i % cols[l];
+        if (l == 3 && col >= outputs) continue;
+        init[z * h->np + h->off_w[l] + i] = a * uhash(seed + 7919ULL * z, (uint64_t)(l * 1000003 + i));
+      }
+    }
+  cudaError_t e = cudaSuccess;
+  auto al = [&](void **p, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+  };
+  al((void **)&h->p, sizeof(float) * n);
+  al((void **)&h->g, sizeof(float) * n);
+  al((void **)&h->m, sizeof(float) * n);
+  al((void **)&h->v, sizeof(float) * n);
+  al((void **)&h->pb, sizeof(bf16) * n);
+  al((void **)&h->d_tmean, sizeof(float) * kOutPad * 3);
+  al((void **)&h->loss, sizeof(float) * ensemble);
+  if (e != cudaSuccess) {
+    cudaFree(h->p);
+    cudaFree(h->g);
+    cudaFree(h->m);
+    cudaFree(h->v);
+    cudaFree(h->pb);
+    cudaFree(h->d_tmean);
+    cudaFree(h->loss);
+    delete h;
+    return fail(CHAOS_LYAP_ENOMEM, std::string("surrogate parameters: ") + cudaGetErrorString(e));
+  }
+  // default frequencies: half-integer multiples along each axis,
+  // sin / cos (pi j u) and (pi j v), j = 1..4
+  for (int j = 0; j < 4; j++) {
+    h->freqs.w[2 * j][0] = 0.5f * (j + 1);
+    h->freqs.w[2 * j][1] = 0.f;
+    h->freqs.w[2 * j + 1][0] = 0.f;
+    h->freqs.w[2 * j + 1][1] = 0.5f * (j + 1);
+  }
+  h->d_tstd = h->d_tmean + kOutPad;
+  h->d_tinv = h->d_tmean + 2 * kOutPad;
+  cudaMemcpy(h->p, init.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
+  cudaMemset(h->g, 0, sizeof(float) * n);
+  cudaMemset(h->m, 0, sizeof(float) * n);
+  cudaMemset(h->v, 0, sizeof(float) * n);
+  to_bf16_kernel<<<blocks(n, 256), 256>>>(h->p, h->pb, n);
+  for (int c = 0; c < kOutPad; c++) h->tmean[c] = 0.f, h->tstd[c] = 1.f;
+  float tb[3 * kOutPad];
+  for (int c = 0; c < kOutPad; c++) tb[c] = 0.f, tb[kOutPad + c] = 1.f, tb[2 * kOutPad + c] = 1.f;
+  cudaMemcpy(h->d_tmean, tb, sizeof tb, cudaMemcpyHostToDevice);
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+    delete h;
+    return cuda_fail(e, "surrogate init");
+  }
+  *out = h;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_mlp_destroy(chaos_mlp *h) {
+  if (!h) return CHAOS_LYAP_OK;
+  DevGuard g(h->device);
+  cudaDeviceSynchronize();
+  free_ws(h);
+  cudaFree(h->p);
+  cudaFree(h->g);
+  cudaFree(h->m);
+  cudaFree(h->v);
+  cudaFree(h->pb);
+  cudaFree(h->d_tmean);
+  cudaFree(h->loss);
+  delete h;
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_mlp_set_domain(chaos_mlp *h, double u0, double u1, double v0, double v1) {
+  if (!h || !(u1 != u0) || !(v1 != v0)) return fail(CHAOS_LYAP_EINVAL, "empty domain");
+  h->u0 = u0;
+  h->us = 1.0 / (u1 - u0);
+  h->v0 = v0;
+  h->vs = 1.0 / (v1 - v0);
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_mlp_set_features(chaos_mlp *h, const float *freqs) {
+  if (!h || !freqs) return fail(CHAOS_LYAP_EINVAL, "null argument");
+  for (int f = 0; f < 8; f++) {
+    h->freqs.w[f][0] = freqs[2 * f];
+    h->freqs.w[f][1] = freqs[2 * f + 1];
+  }
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_mlp_set_target_scale(chaos_mlp *h, const float *mean, const float *stdev) {
+  if (!h || !mean || !stdev) return fail(CHAOS_LYAP_EINVAL, "null argument");
+  float tb[3 * kOutPad];
+  for (int c = 0; c < kOutPad; c++) {
+    const bool used = c < h->outs;
+    h->tmean[c] = used ? mean[c] : 0.f;
+    h->tstd[c] = used ? std::max(stdev[c], 1e-12f) : 1.f;
+    tb[c] = h->tmean[c];
+    tb[kOutPad + c] = h->tstd[c];
+    tb[2 * kOutPad + c] = 1.f / h->tstd[c];
+  }
+  DevGuard g(h->device);
+  cudaError_t e = cudaMemcpy(h->d_tmean, tb, sizeof tb, cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "set_target_scale");
+}
+
+int64_t chaos_mlp_num_params(chaos_mlp *h) { return h ? h->np * h->E : -1; }
+
+// FP32 master parameters (E x np) to / from host memory.
+int chaos_mlp_get_params(chaos_mlp *h, float *host) {
+  if (!h || !host) return fail(CHAOS_LYAP_EINVAL, "null argument");
+  DevGuard g(h->device);
+  cudaError_t e = cudaMemcpy(host, h->p, sizeof(float) * h->np * h->E, cudaMemcpyDeviceToHost);
+  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "get_params");
+}
+int chaos_mlp_set_params(chaos_mlp *h, const float *host) {
+  if (!h || !host) return fail(CHAOS_LYAP_EINVAL, "null argument");
+  DevGuard g(h->device);
+  const int64_t n = h->np * h->E;
+  cudaError_t e = cudaMemcpy(h->p, host, sizeof(float) * n, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_fail(e, "set_params");
+  to_bf16_kernel<<<blocks(n, 256), 256>>>(h->p, h->pb, n);
+  e = cudaDeviceSynchronize();
+  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "set_params");
+}
+
+// Loss gradient of every network on `rows` points (device xy: rows x 2
+// doubles, T: rows x outputs doubles), copied to host (E x np floats); the
+// per-network losses into loss_out (E floats).  No parameter update.
+int chaos_mlp_gradient(chaos_mlp *h, const double *xy, const double *T, int64_t rows,
+                       float *grads_out, float *loss_out) {
+  if (!h || !xy || !T || rows <= 0) return fail(CHAOS_LYAP_EINVAL, "bad arguments");
+  DevGuard g(h->device);
+  int rc = ensure_ws(h, rows);
+  if (rc) return rc;
+  std::vector<double> td(rows * h->outs);
+  cudaMemcpy(td.data(), T, sizeof(double) * td.size(), cudaMemcpyDeviceToHost);
+  std::vector<float> tf(td.begin(), td.end());
+  cudaMemcpy(h->Tb, tf.data(), sizeof(float) * tf.size(), cudaMemcpyHostToDevice);
+  rc = grad_step(h, xy, h->Tb, rows, 0);
+  if (rc) return cuda_fail((cudaError_t)rc, "gradient");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "gradient");
+  if (grads_out) cudaMemcpy(grads_out, h->g, sizeof(float) * h->np * h->E, cudaMemcpyDeviceToHost);
+  if (loss_out) cudaMemcpy(loss_out, h->loss, sizeof(float) * h->E, cudaMemcpyDeviceToHost);
+  return CHAOS_LYAP_OK;
+}
+
+// Adam training on N points (device xy: N x 2, T: N x outputs doubles):
+// `steps` mini-batches of `batch` rows drawn without replacement per epoch
+// from a seeded permutation (a different one per call seed); lr, betas
+// (0.9, 0.999), eps 1e-8.  Every network sees the same batches.  The last
+// step's per-network losses go to loss_out (E floats, may be NULL).
+int chaos_mlp_train(chaos_mlp *h, const double *xy, const double *T, int64_t N, int steps,
+                    int batch, float lr, uint64_t seed, void *stream, float *loss_out) {
+  if (!h || !xy || !T || N <= 0 || steps < 0 || batch < 16)
+    return fail(CHAOS_LYAP_EINVAL, "bad arguments");
+  DevGuard g(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t B = std::min<int64_t>(batch, N);
+  int rc = ensure_ws(h, B);
+  if (rc) return rc;
+  // targets to FP32 on the host once, gathered per batch (small: N x 3)
+  std::vector<double> xd(N * 2), td(N * h->outs);
+  cudaMemcpyAsync(xd.data(), xy, sizeof(double) * xd.size(), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(td.data(), T, sizeof(double) * td.size(), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  std::vector<int64_t> perm(N);
+  for (int64_t i = 0; i < N; i++) perm[i] = i;
+  uint64_t st = seed * 0x9E3779B97F4A7C15ULL + 1;
+  auto rnd = [&]() {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    return st;
+  };
+  int64_t pos = N;
+  std::vector<double> bx(B * 2);
+  std::vector<float> bt(B * h->outs);
+  const int64_t n = h->np * h->E;
+  for (int it = 0; it < steps; it++) {
+    for (int64_t r = 0; r < B; r++) {
+      if (pos >= N) {  // new epoch: Fisher-Yates shuffle
+        for (int64_t i = N - 1; i > 0; i--) std::swap(perm[i], perm[rnd() % (uint64_t)(i + 1)]);
+        pos = 0;
+      }
+      const int64_t j = perm[pos++];
+      bx[2 * r] = xd[2 * j];
+      bx[2 * r + 1] = xd[2 * j + 1];
+      for (int c = 0; c < h->outs; c++) bt[r * h->outs + c] = (float)td[j * h->outs + c];
+    }
+    cudaMemcpyAsync(h->xyb, bx.data(), sizeof(double) * B * 2, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(h->Tb, bt.data(), sizeof(float) * B * h->outs, cudaMemcpyHostToDevice, s);
+    rc = grad_step(h, h->xyb, h->Tb, B, s);
+    if (rc) return cuda_fail((cudaError_t)rc, "train step");
+    h->t++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f / (1.f - std::pow(b1, (float)h->t));
+    const float c2 = 1.f / (1.f - std::pow(b2, (float)h->t));
+    adam_kernel<<<blocks(n, 256), 256, 0, s>>>(h->p, h->g, h->m, h->v, h->pb, n, lr, b1, b2, 1e-8f, c1, c2);
+    // the host buffers are reused next step: wait for the copies to be consumed
+    cudaStreamSynchronize(s);
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "train");
+  if (loss_out && steps > 0) cudaMemcpy(loss_out, h->loss, sizeof(float) * h->E, cudaMemcpyDeviceToHost);
+  return CHAOS_LYAP_OK;
+}
+
+// Ensemble prediction on N points (device xy: N x 2 doubles): mean and
+// standard deviation over the networks, de-standardised, N x outputs floats
+// each (either may be NULL).  Processes `chunk` points at a time.
+int chaos_mlp_predict(chaos_mlp *h, const double *xy, int64_t N, float *mean, float *stdev,
+                      void *stream) {
+  if (!h || !xy || N < 0) return fail(CHAOS_LYAP_EINVAL, "bad arguments");
+  DevGuard g(h->device);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t chunk = std::min<int64_t>(N, 1 << 16);
+  int rc = ensure_ws(h, std::max<int64_t>(chunk, 1));
+  if (rc) return rc;
+  for (int64_t o = 0; o < N; o += chunk) {
+    const int64_t rows = std::min(chunk, N - o);
+    features_kernel<<<blocks(rows, 256), 256, 0, s>>>(xy + 2 * o, rows, h->u0, h->us, h->v0,
+                                                      h->vs, h->freqs, h->X);
+    rc = forward(h, rows, s);
+    if (rc) return cuda_fail((cudaError_t)rc, "predict");
+    output_kernel<<<dim3(blocks(rows, 128), 1, h->E), 128, 0, s>>>(
+        h->Y, h->p + h->off_b[3], h->np, rows, h->outs, nullptr, nullptr, nullptr, nullptr, nullptr);
+    ensemble_kernel<<<blocks(rows, 128), 128, 0, s>>>(
+        h->Y, h->E, rows, h->outs, h->d_tmean, h->d_tstd, mean ? mean + o * h->outs : nullptr,
+        stdev ? stdev + o * h->outs : nullptr);
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "predict");
+}
+
+}  // extern "C"

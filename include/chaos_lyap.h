@@ -253,6 +253,12 @@ int chaos_lyap_make_inits(int32_t dim, int64_t P, const double *base, double amp
  * reference reports whole-run wall time only, raiitimer.h). */
 int chaos_lyap_fma_peak(int device, int precision, double seconds, double *tflops);
 
+/* The same initial states for an arbitrary list of point indices: out[i] is
+ * what chaos_lyap_make_inits writes for point index[i] (used to integrate a
+ * scattered subset of a large grid, e.g. the cells a surrogate flags). */
+int chaos_lyap_make_inits_at(int32_t dim, int64_t count, const int64_t *index, const double *base,
+                             double amp, int32_t dist, uint64_t seed, double *out);
+
 #ifdef __cplusplus
 }
 #endif

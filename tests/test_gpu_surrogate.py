@@ -1,0 +1,87 @@
+"""The surrogate's own GPU kernels: loss gradients against the CPU FP64
+backpropagation (oracle/mlp_oracle.py), training, and the refined map
+against the plain sweep on held-out cells."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+DOM = (5.0, 20.0, 0.0, 200.0)
+
+
+def _batch(n, seed=0):
+    rng = np.random.default_rng(seed)
+    xy = np.stack([rng.uniform(5, 20, n), rng.uniform(0, 200, n)], 1)
+    # a smooth stand-in for a spectrum
+    T = np.stack([np.tanh((xy[:, 1] - 30) / 20) * 0.9, 0.05 * np.sin(xy[:, 0]),
+                  -(xy[:, 0] + 1 + 8 / 3) - 0.9 * np.tanh((xy[:, 1] - 30) / 20)], 1)
+    return xy, T
+
+
+def test_gradients_match_cpu_backprop(lib):
+    import torch
+    from chaos_oneapi_b200.surrogate import MLPEnsemble
+    net = MLPEnsemble(ensemble=2, width=128, outputs=3, seed=3)
+    net.set_domain(*DOM)
+    xy, T = _batch(256)
+    tm, ts = T.mean(0), T.std(0)
+    net.set_target_scale(tm, ts)
+    g, loss = net.gradient(torch.from_numpy(xy).cuda(), torch.from_numpy(T).cuda())
+    params = net.get_params()
+    for e in range(2):
+        l_cpu, g_cpu = mo.loss_and_grad(params[e].astype(np.float64), 128, xy, T, tm, ts, DOM)
+        ge = g[e].astype(np.float64)
+        rel = np.linalg.norm(ge - g_cpu) / np.linalg.norm(g_cpu)
+        cos = ge @ g_cpu / (np.linalg.norm(ge) * np.linalg.norm(g_cpu))
+        # BF16 activations on the GPU, FP64 on the CPU
+        assert rel < 5e-2 and cos > 0.998, (e, rel, cos)
+        assert abs(loss[e] - l_cpu) < 2e-2 * max(1.0, l_cpu)
+    net.close()
+
+
+def test_training_fits_a_smooth_map(lib):
+    import torch
+    from chaos_oneapi_b200.surrogate import MLPEnsemble
+    net = MLPEnsemble(ensemble=4, width=128, outputs=3, seed=1)
+    net.set_domain(*DOM)
+    xy, T = _batch(8192, 1)
+    net.set_target_scale(T.mean(0), T.std(0))
+    dxy, dT = torch.from_numpy(xy).cuda(), torch.from_numpy(T).cuda()
+    first = net.train(dxy, dT, steps=1, batch=1024)
+    last = net.train(dxy, dT, steps=1500, batch=1024, seed=2)
+    assert (last < first / 20).all(), (first, last)
+    xh, Th = _batch(2048, 7)
+    mean, std = net.predict(torch.from_numpy(xh).cuda())
+    err = np.abs(mean.cpu().numpy() - Th)
+    assert err[:, 0].mean() < 0.05 and err[:, 2].mean() < 0.2
+    assert std.cpu().numpy()[:, 0].mean() < 0.05
+    net.close()
+
+
+def test_refined_map_against_plain_on_held_out_cells(lib):
+    """A 256 x 256 Lorenz map (short horizon): the refined map integrates a
+    fraction of the cells and agrees with the plain sweep on the regime of
+    held-out cells."""
+    from chaos_oneapi_b200.surrogate import MapSpec, RefineConfig, plain_sweep, refine_map
+    spec = MapSpec("lorenz", [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, 256], [1, 0.0, 200.0, 256],
+                   [1.0, 1.0, 1.0], seed=4)
+    sw = lib.Sweep(model="lorenz", method="var", integrator="dverk65", precision="fp64",
+                   rtol=1e-8, atol=1e-8, h=1e-3, t_transient=20.0, t_avg=300.0, dt_renorm=1.0)
+    cfg = RefineConfig(train_grid=64, steps0=3000, steps_round=1500, rounds=2, round_grid_step=2,
+                       round_max_new=8192)
+    out, mask, info = refine_map(spec, sw, cfg)
+    rng = np.random.default_rng(11)
+    held = rng.choice(256 * 256, 1000, replace=False)
+    truth, st = plain_sweep(sw, spec, held)
+    ok = st == 0
+    agree = ((out[held, 0] > 0.01) == (truth[:, 0] > 0.01))[ok].mean()
+    # the trained ensemble fills part of the map (the rest, flagged by the
+    # spread / near-zero rule, is integrated), and the regimes it fills agree
+    assert info["plain_fraction"] < 0.95, info
+    assert agree > 0.98, (agree, info)
+    filled = ok & ~mask[held]
+    assert filled.sum() > 20
+    assert np.median(np.abs(out[held][filled, 0] - truth[filled, 0])) < 0.05
+    sw.close()
