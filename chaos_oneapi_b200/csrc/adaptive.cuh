@@ -19,6 +19,8 @@
 //    precision, at intervals of at most dt_renorm and exactly at the phase
 //    ends; log-norms summed in FP64 with Kahan compensation.
 #pragma once
+#include <type_traits>
+
 #include "kernels.h"
 #include "models.cuh"
 
@@ -84,118 +86,188 @@ CL_HD float fast_div(float a, float b) {
   return a / b;
 #endif
 }
-template <class R>
-CL_HD float err_term(R y0, R y1, R e, float rtol, float atol) {
-  const float m = fmaxf(fabsf((float)y0), fabsf((float)y1));
-  const float r = fast_div((float)e, fmaf(rtol, m, atol));
-  return r * r;
+
+// ------------------------------------------------- element arithmetic
+// The RK passes below are written over an element type E: float or double
+// (one row of the joint system per pass), or float2 (two rows side by side,
+// advanced by the packed FP32 instructions of sm_100: one FFMA2 performs the
+// multiply-add of both rows).  Coefficients and h are scalars of type S.
+// Every stage combination is an explicit chain mul, fma, fma, ... so the
+// scalar and packed forms do the same operations in the same order.
+template <class E> struct ScalarOf { using type = E; };
+template <> struct ScalarOf<float2> { using type = float; };
+
+CL_HD float vmul(float a, float b) { return a * b; }
+CL_HD double vmul(double a, double b) { return a * b; }
+CL_HD float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+CL_HD double vfma(double a, double b, double c) { return fma(a, b, c); }
+CL_HD float2 vmul(float a, float2 b) {
+#ifdef __CUDA_ARCH__
+  return __fmul2_rn(make_float2(a, a), b);
+#else
+  return make_float2(a * b.x, a * b.y);
+#endif
+}
+CL_HD float2 vfma(float a, float2 b, float2 c) {
+#ifdef __CUDA_ARCH__
+  return __ffma2_rn(make_float2(a, a), b, c);
+#else
+  return make_float2(fmaf(a, b.x, c.x), fmaf(a, b.y, c.y));
+#endif
+}
+CL_HD float2 vmul2(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+  return __fmul2_rn(a, b);
+#else
+  return make_float2(a.x * b.x, a.y * b.y);
+#endif
+}
+CL_HD float2 vfma2(float2 a, float2 b, float2 c) {
+#ifdef __CUDA_ARCH__
+  return __ffma2_rn(a, b, c);
+#else
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
 }
 
-// One DVERK 6(5) pass over an N-vector y: y1 = 6th-order solution, err2 +=
-// sum of squared weighted error components.  fn(s, arg, out) evaluates the
-// derivative of stage s (0-based) at arg.
-template <int N, class R, class F>
-CL_HD void dverk_pass(const R *y, R h, const F &fn, R *y1, float &err2,
-                                           float rtol, float atol) {
-  R k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
+// lin(c1, k1, c2, k2, ...) = c1 k1 + c2 k2 + ... (left to right)
+template <class S, class E> CL_HD E lin_acc(E acc) { return acc; }
+// (arguments by value: the coefficients are constexpr members, which device
+// code may read but not bind to a reference)
+template <class S, class E, class... Rest>
+CL_HD E lin_acc(E acc, double c, E k, Rest... rest) {
+  return lin_acc<S, E>(vfma(S(c), k, acc), rest...);
+}
+template <class S, class E, class... Rest>
+CL_HD E lin(double c, E k, Rest... rest) {
+  return lin_acc<S, E>(vmul(S(c), k), rest...);
+}
+
+// Squared weighted error e / (atol + rtol max(|y0|, |y1|)) accumulated per
+// row: a float accumulator for a scalar row, a float2 for a packed pair.
+template <class E> struct ErrAcc { using type = float; };
+template <> struct ErrAcc<float2> { using type = float2; };
+
+template <class R>
+CL_HD void err_acc(R y0, R y1, R e, float rtol, float atol, float &acc) {
+  const float m = fmaxf(fabsf((float)y0), fabsf((float)y1));
+  const float r = fast_div((float)e, fmaf(rtol, m, atol));
+  acc = fmaf(r, r, acc);
+}
+// The pair shares one reciprocal: 1 / (s_x s_y) scaled by the other weight.
+CL_HD void err_acc(float2 y0, float2 y1, float2 e, float rtol, float atol, float2 &acc) {
+  const float sx = fmaf(rtol, fmaxf(fabsf(y0.x), fabsf(y1.x)), atol);
+  const float sy = fmaf(rtol, fmaxf(fabsf(y0.y), fabsf(y1.y)), atol);
+  const float inv = fast_div(1.0f, sx * sy);
+  const float2 r = vmul2(e, make_float2(sy * inv, sx * inv));
+  acc = vfma2(r, r, acc);
+}
+
+// One DVERK 6(5) pass over an N-vector y of elements E: y1 = 6th-order
+// solution, err2 += squared weighted error components.  fn(s, arg, out)
+// evaluates the derivative of stage s (0-based) at arg.
+template <int N, class E, class F>
+CL_HD void dverk_pass(const E *y, typename ScalarOf<E>::type h, const F &fn, E *y1,
+                      typename ErrAcc<E>::type &err2, float rtol, float atol) {
+  using S = typename ScalarOf<E>::type;
   using T = DV;
+  E k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
   fn(0, y, k1);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = y[j] + h * (C<R>(T::a21) * k1[j]);
+  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
   fn(1, arg, k2);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = y[j] + h * (C<R>(T::a31) * k1[j] + C<R>(T::a32) * k2[j]);
+  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
   fn(2, arg, k3);
 #pragma unroll
   for (int j = 0; j < N; j++)
-    arg[j] = y[j] + h * (C<R>(T::a41) * k1[j] + C<R>(T::a42) * k2[j] + C<R>(T::a43) * k3[j]);
+    arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
   fn(3, arg, k4);
 #pragma unroll
   for (int j = 0; j < N; j++)
-    arg[j] = y[j] + h * (C<R>(T::a51) * k1[j] + C<R>(T::a52) * k2[j] + C<R>(T::a53) * k3[j] +
-                         C<R>(T::a54) * k4[j]);
+    arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
   fn(4, arg, k5);
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    arg[j] = y[j] + h * (C<R>(T::a61) * k1[j] + C<R>(T::a62) * k2[j] + C<R>(T::a63) * k3[j] +
-                         C<R>(T::a64) * k4[j] + C<R>(T::a65) * k5[j]);
-    acc[j] = C<R>(T::b1) * k1[j] + C<R>(T::b3) * k3[j] + C<R>(T::b4) * k4[j] + C<R>(T::b5) * k5[j];
-    e[j] = C<R>(T::d1) * k1[j] + C<R>(T::d3) * k3[j] + C<R>(T::d4) * k4[j] + C<R>(T::d5) * k5[j];
+    arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                            T::a65, k5[j]), y[j]);
+    acc[j] = lin<S>(T::b1, k1[j], T::b3, k3[j], T::b4, k4[j], T::b5, k5[j]);
+    e[j] = lin<S>(T::d1, k1[j], T::d3, k3[j], T::d4, k4[j], T::d5, k5[j]);
   }
   {
-    R k6[N];
+    E k6[N];
     fn(5, arg, k6);
 #pragma unroll
-    for (int j = 0; j < N; j++) e[j] += C<R>(T::d6) * k6[j];
+    for (int j = 0; j < N; j++) e[j] = vfma(S(T::d6), k6[j], e[j]);
   }
 #pragma unroll
   for (int j = 0; j < N; j++)
-    arg[j] = y[j] + h * (C<R>(T::a71) * k1[j] + C<R>(T::a72) * k2[j] + C<R>(T::a73) * k3[j] +
-                         C<R>(T::a74) * k4[j] + C<R>(T::a75) * k5[j]);
+    arg[j] = vfma(h, lin<S>(T::a71, k1[j], T::a72, k2[j], T::a73, k3[j], T::a74, k4[j],
+                            T::a75, k5[j]), y[j]);
   fn(6, arg, k7);
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    arg[j] = y[j] + h * (C<R>(T::a81) * k1[j] + C<R>(T::a82) * k2[j] + C<R>(T::a83) * k3[j] +
-                         C<R>(T::a84) * k4[j] + C<R>(T::a85) * k5[j] + C<R>(T::a87) * k7[j]);
-    acc[j] += C<R>(T::b7) * k7[j];
-    e[j] += C<R>(T::d7) * k7[j];
+    arg[j] = vfma(h, lin<S>(T::a81, k1[j], T::a82, k2[j], T::a83, k3[j], T::a84, k4[j],
+                            T::a85, k5[j], T::a87, k7[j]), y[j]);
+    acc[j] = vfma(S(T::b7), k7[j], acc[j]);
+    e[j] = vfma(S(T::d7), k7[j], e[j]);
   }
   {
-    R k8[N];
+    E k8[N];
     fn(7, arg, k8);
 #pragma unroll
     for (int j = 0; j < N; j++) {
-      acc[j] += C<R>(T::b8) * k8[j];
-      e[j] += C<R>(T::d8) * k8[j];
-      y1[j] = y[j] + h * acc[j];
-      err2 += err_term<R>(y[j], y1[j], h * e[j], rtol, atol);
+      acc[j] = vfma(S(T::b8), k8[j], acc[j]);
+      e[j] = vfma(S(T::d8), k8[j], e[j]);
+      y1[j] = vfma(h, acc[j], y[j]);
+      err_acc(y[j], y1[j], vmul(h, e[j]), rtol, atol, err2);
     }
   }
 }
 
 // One Dopri5 pass: k1 = derivative at y (FSAL, given), y1 = 5th-order
 // solution, k7 = derivative at y1 (the next step's k1).
-template <int N, class R, class F>
-CL_HD void dopri_pass(const R *y, const R *k1, R h, const F &fn, R *y1, R *k7,
-                                           float &err2, float rtol, float atol) {
-  R k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
+template <int N, class E, class F>
+CL_HD void dopri_pass(const E *y, const E *k1, typename ScalarOf<E>::type h, const F &fn,
+                      E *y1, E *k7, typename ErrAcc<E>::type &err2, float rtol, float atol) {
+  using S = typename ScalarOf<E>::type;
   using T = DP;
+  E k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = y[j] + h * (C<R>(T::a21) * k1[j]);
+  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
   fn(1, arg, k2);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = y[j] + h * (C<R>(T::a31) * k1[j] + C<R>(T::a32) * k2[j]);
+  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
   fn(2, arg, k3);
 #pragma unroll
   for (int j = 0; j < N; j++)
-    arg[j] = y[j] + h * (C<R>(T::a41) * k1[j] + C<R>(T::a42) * k2[j] + C<R>(T::a43) * k3[j]);
+    arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
   fn(3, arg, k4);
 #pragma unroll
   for (int j = 0; j < N; j++)
-    arg[j] = y[j] + h * (C<R>(T::a51) * k1[j] + C<R>(T::a52) * k2[j] + C<R>(T::a53) * k3[j] +
-                         C<R>(T::a54) * k4[j]);
+    arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
   fn(4, arg, k5);
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    arg[j] = y[j] + h * (C<R>(T::a61) * k1[j] + C<R>(T::a62) * k2[j] + C<R>(T::a63) * k3[j] +
-                         C<R>(T::a64) * k4[j] + C<R>(T::a65) * k5[j]);
-    e[j] = C<R>(T::e1) * k1[j] + C<R>(T::e3) * k3[j] + C<R>(T::e4) * k4[j] + C<R>(T::e5) * k5[j];
-    y1[j] = C<R>(T::a71) * k1[j] + C<R>(T::a73) * k3[j] + C<R>(T::a74) * k4[j] + C<R>(T::a75) * k5[j];
+    arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                            T::a65, k5[j]), y[j]);
+    e[j] = lin<S>(T::e1, k1[j], T::e3, k3[j], T::e4, k4[j], T::e5, k5[j]);
+    y1[j] = lin<S>(T::a71, k1[j], T::a73, k3[j], T::a74, k4[j], T::a75, k5[j]);
   }
   {
-    R k6[N];
+    E k6[N];
     fn(5, arg, k6);
 #pragma unroll
     for (int j = 0; j < N; j++) {
-      y1[j] = y[j] + h * (y1[j] + C<R>(T::a76) * k6[j]);
-      e[j] += C<R>(T::e6) * k6[j];
+      y1[j] = vfma(h, vfma(S(T::a76), k6[j], y1[j]), y[j]);
+      e[j] = vfma(S(T::e6), k6[j], e[j]);
     }
   }
   fn(6, y1, k7);
 #pragma unroll
   for (int j = 0; j < N; j++) {
-    e[j] += C<R>(T::e7) * k7[j];
-    err2 += err_term<R>(y[j], y1[j], h * e[j], rtol, atol);
+    e[j] = vfma(S(T::e7), k7[j], e[j]);
+    err_acc(y[j], y1[j], vmul(h, e[j]), rtol, atol, err2);
   }
 }
 
@@ -281,27 +353,129 @@ struct Lane {
   int64_t pt;
 };
 
+// Packed FP32 form (odd k): the rows of the joint system -- the state and
+// the k tangent vectors -- advance two at a time as float2 pairs:
+// (state, v_{k-1}) in one pass, which also records the stage points, then
+// (v_0, v_1), (v_2, v_3), ... at those stage points.  Each stage combination
+// of two rows is then one packed multiply-add per coefficient instead of two.
+template <class M, int K, class R>
+struct Packed {
+  static constexpr bool value = std::is_same<R, float>::value && (K % 2 == 1);
+};
+
+template <class M>
+struct PairStateStages {  // (state, last tangent vector)
+  const float *p;
+  float (*X)[M::N];
+  CL_HD void operator()(int s, const float2 *arg, float2 *out) const {
+    constexpr int N = M::N;
+    float ax[N], av[N], ox[N], ov[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      ax[j] = arg[j].x;
+      av[j] = arg[j].y;
+    }
+    if (s > 0) {
+#pragma unroll
+      for (int j = 0; j < N; j++) X[s][j] = ax[j];
+    }
+    M::f(ax, ox, p);
+    M::jv(av, ov, p, ax);
+#pragma unroll
+    for (int j = 0; j < N; j++) out[j] = make_float2(ox[j], ov[j]);
+  }
+};
+template <class M>
+struct PairTangentStages {  // two tangent vectors at the recorded stage points
+  const float *p;
+  const float *x0;
+  const float (*X)[M::N];
+  CL_HD void operator()(int s, const float2 *arg, float2 *out) const {
+    constexpr int N = M::N;
+    const float *xs = s == 0 ? x0 : X[s];
+    float a0[N], a1[N], o0[N], o1[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      a0[j] = arg[j].x;
+      a1[j] = arg[j].y;
+    }
+    M::jv(a0, o0, p, xs);
+    M::jv(a1, o1, p, xs);
+#pragma unroll
+    for (int j = 0; j < N; j++) out[j] = make_float2(o0[j], o1[j]);
+  }
+};
+
 // Attempt one step of length h; the tangent vectors only when `joint`.
 template <class M, int K, class R, int INTEG>
 CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol, float atol,
                     R (&x1)[M::N], R (&V1)[K][M::N], R (&kx1)[M::N], R (&kv1)[K][M::N]) {
   constexpr int N = M::N;
   constexpr int S = (INTEG == kDverk65) ? 8 : 7;
-  R X[S][N];
-  float err2 = 0.f;
-  StateStages<M, R> fs{st.p, X};
-  if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
-  else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
-  if (joint) {
-    TangentStages<M, R> ft{st.p, st.x, X};
-#pragma unroll
-    for (int i = 0; i < K; i++) {
-      if (INTEG == kDverk65) dverk_pass<N, R>(st.V[i], h, ft, V1[i], err2, rtol, atol);
-      else dopri_pass<N, R>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
-    }
-  }
   const float inv_nc = joint ? 1.0f / (N * (1 + K)) : 1.0f / N;
-  return sqrtf(err2 * inv_nc);  // err2 >= 0
+  R X[S][N];
+  if constexpr (Packed<M, K, R>::value) {
+    float2 ya[N], ka[N], ya1[N], ka1[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      ya[j] = make_float2(st.x[j], st.V[K - 1][j]);
+      ka[j] = make_float2(st.kx[j], st.kv[K - 1][j]);
+    }
+    float2 ea = make_float2(0.f, 0.f);
+    PairStateStages<M> fa{st.p, X};
+    if (INTEG == kDverk65) dverk_pass<N, float2>(ya, h, fa, ya1, ea, rtol, atol);
+    else dopri_pass<N, float2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      x1[j] = ya1[j].x;
+      V1[K - 1][j] = ya1[j].y;
+      if (INTEG == kDopri5) {
+        kx1[j] = ka1[j].x;
+        kv1[K - 1][j] = ka1[j].y;
+      }
+    }
+    float err2 = ea.x;
+    if (joint) {
+      float2 eb = make_float2(0.f, 0.f);
+      PairTangentStages<M> fb{st.p, st.x, X};
+#pragma unroll
+      for (int m = 0; m + 1 < K; m += 2) {
+        float2 yb[N], kb[N], yb1[N], kb1[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+          yb[j] = make_float2(st.V[m][j], st.V[m + 1][j]);
+          kb[j] = make_float2(st.kv[m][j], st.kv[m + 1][j]);
+        }
+        if (INTEG == kDverk65) dverk_pass<N, float2>(yb, h, fb, yb1, eb, rtol, atol);
+        else dopri_pass<N, float2>(yb, kb, h, fb, yb1, kb1, eb, rtol, atol);
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+          V1[m][j] = yb1[j].x;
+          V1[m + 1][j] = yb1[j].y;
+          if (INTEG == kDopri5) {
+            kv1[m][j] = kb1[j].x;
+            kv1[m + 1][j] = kb1[j].y;
+          }
+        }
+      }
+      err2 += ea.y + (eb.x + eb.y);
+    }
+    return sqrtf(err2 * inv_nc);
+  } else {
+    float err2 = 0.f;
+    StateStages<M, R> fs{st.p, X};
+    if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
+    else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
+    if (joint) {
+      TangentStages<M, R> ft{st.p, st.x, X};
+#pragma unroll
+      for (int i = 0; i < K; i++) {
+        if (INTEG == kDverk65) dverk_pass<N, R>(st.V[i], h, ft, V1[i], err2, rtol, atol);
+        else dopri_pass<N, R>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
+      }
+    }
+    return sqrtf(err2 * inv_nc);  // err2 >= 0
+  }
 }
 
 // Gram-Schmidt in FP64 on the k tangent vectors; r[i] = norms after the
@@ -434,6 +608,12 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
     L.sum[i] = L.comp[i] = 0.0;
     L.prod[i] = 1.0;
   }
+  // The tangent rows ride along in the packed transient pass; start them
+  // from zero so that they stay finite until the alignment phase sets them.
+#pragma unroll
+  for (int i = 0; i < K; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) L.V[i][j] = L.kv[i][j] = R(0);
   if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
   if (a.t_transient > 0) {
     L.phase = kTransient;
