@@ -88,6 +88,11 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Starts sampling and returns once the first sample has arrived:
+        nvidia-smi's start-up (NVML initialisation) stalls CUDA launches of
+        other processes for ~0.1 s, which must not fall inside a timed region.
+        Only samples taken after this returns are reported."""
+        self.mark = 0
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
@@ -97,6 +102,12 @@ class ClockSampler:
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        time.sleep(0.05)
+        self.mark = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -112,7 +123,9 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples from the timed region (all of them if it was shorter than one period)
+        lines = self.lines[self.mark:] or self.lines
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 7:
                 continue

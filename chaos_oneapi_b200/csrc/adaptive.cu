@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(128, MINB) sweep_kernel(const AdaptiveArgs a) 
     }
     const bool due = active && L.phase != kTransient && L.t_gs >= L.L;
     if (__any_sync(0xffffffffu, due)) {
-      if (active && L.phase != kTransient && L.t_gs > 0.0 && !lane_gram_schmidt(L, a, c)) {
+      if (active && L.phase != kTransient && L.t_gs > 0.f && !lane_gram_schmidt(L, a, c)) {
         lane_finish(L, a, 1);
         pt = a.queue ? next_point(a) : a.P;
         active = pt < a.P;
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 3 : 1) batch_kernel(cons
     });
     if (__any_sync(0xffffffffu, due) && active) {
       const bool failed = visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-        if (L.phase == kTransient || !(L.t_gs > 0.0)) return false;
+        if (L.phase == kTransient || !(L.t_gs > 0.f)) return false;
         if (lane_gram_schmidt(L, b.seg[wseg], c)) return false;
         lane_finish(L, b.seg[wseg], 1);
         return true;

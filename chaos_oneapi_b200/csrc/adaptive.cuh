@@ -15,9 +15,10 @@
 //    arithmetic as one RK step of the joint (n + k n)-dimensional system, with
 //    a register footprint of one vector's stages instead of all of them.
 //  * Renormalisation (see Lane): Gram-Schmidt (classical as
-//    cuda/tools/linalg.dp.cpp:36-51, or modified) in FP64 whatever the state
-//    precision, at intervals of at most dt_renorm and exactly at the phase
-//    ends; log-norms summed in FP64 with Kahan compensation.
+//    cuda/tools/linalg.dp.cpp:36-51, or modified) in the precision of the
+//    tangent vectors, at intervals of at most dt_renorm (short enough that
+//    little of any vector cancels) and exactly at the phase ends; norms
+//    multiplied and log-norms summed in FP64 with Kahan compensation.
 #pragma once
 #include <type_traits>
 
@@ -300,6 +301,14 @@ enum LaneResult : int32_t { kRunning = 0, kFinished = 1 };
 
 constexpr int kRenormSplitInit = 16, kRenormSplitMax = 64;
 
+// Step-size controller constants (dopri.dp.cpp:9-12: safety 0.9, the step
+// may shrink by at most 1 / facc1 = 0.2 and grow by 1 / facc2 = 10, previous
+// error floored at 1e-4), as base-2 logarithms.
+constexpr float kLog2Safe = -0.15200309344504997f;   // log2 0.9
+constexpr float kLog2Facc1 = 2.321928094887362f;     // log2 5
+constexpr float kLog2Facc2 = -3.321928094887362f;    // log2 0.1
+constexpr float kLog2FacMin = -13.287712379549449f;  // log2 1e-4
+
 // Largest log of the Gram-Schmidt cancellation factor (|v_i| / r_i) allowed
 // between two renormalisations: 0.3 ln(1 / max(rtol, unit roundoff of R)).
 template <class R> CL_HD float renorm_spread_limit(float rtol) {
@@ -340,12 +349,12 @@ struct Lane {
   R kx[N];      // Dopri5 FSAL: derivative of the state
   R kv[K][N];   // Dopri5 FSAL: derivatives of the tangent vectors
   R h;
-  float fac_old;
+  float lfac_old;  // log2 of the previous accepted step's error (>= log2 1e-4)
   int32_t phase;
   bool reject;
   double t_phase, phase_len;  // time into the current phase, its length
-  double t_gs, L;             // time since the last Gram-Schmidt, its target
-  double rate_max;            // largest recent log-cancellation per unit time
+  float t_gs, L;              // time since the last Gram-Schmidt, its target
+  float rate_max;             // largest recent log-cancellation per unit time
   double t_avg;
   double sum[K], comp[K];     // Kahan-compensated sums of log-norms
   double prod[K];             // product of the norms since the last log
@@ -407,6 +416,7 @@ struct PairTangentStages {  // two tangent vectors at the recorded stage points
 };
 
 // Attempt one step of length h; the tangent vectors only when `joint`.
+// Returns the mean square of the weighted error components (err^2).
 template <class M, int K, class R, int INTEG>
 CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol, float atol,
                     R (&x1)[M::N], R (&V1)[K][M::N], R (&kx1)[M::N], R (&kv1)[K][M::N]) {
@@ -460,7 +470,7 @@ CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol,
       }
       err2 += ea.y + (eb.x + eb.y);
     }
-    return sqrtf(err2 * inv_nc);
+    return err2 * inv_nc;
   } else {
     float err2 = 0.f;
     StateStages<M, R> fs{st.p, X};
@@ -474,63 +484,71 @@ CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol,
         else dopri_pass<N, R>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
       }
     }
-    return sqrtf(err2 * inv_nc);  // err2 >= 0
+    return err2 * inv_nc;
   }
 }
 
-// Gram-Schmidt in FP64 on the k tangent vectors; r[i] = norms after the
-// projections (the R diagonal), returns max_i |v_i|^2 / r_i^2: how much of
-// each vector cancelled, i.e. the factor by which errors in the vectors grew
-// relative to what is left of them.
+// Gram-Schmidt on the k tangent vectors in the precision R of the vectors;
+// r[i] = norms after the projections (the R diagonal).  Returns
+// max_i |v_i|^2 / r_i^2: how much of each vector cancelled, i.e. the factor
+// by which errors in the vectors grew relative to what is left of them.
+// Renormalisation keeps that factor near e^(tau / 8), so the projections lose
+// at most a bit or two of R; the log-norms are summed in FP64 by the caller.
+CL_HD float vrsqrt(float s) {
+#ifdef __CUDA_ARCH__
+  return rsqrtf(s);
+#else
+  return 1.0f / sqrtf(s);
+#endif
+}
+CL_HD double vrsqrt(double s) {
+#ifdef __CUDA_ARCH__
+  return rsqrt(s);
+#else
+  return 1.0 / sqrt(s);
+#endif
+}
+
 template <int N, int K, class R>
-CL_HD double renormalise(R (&V)[K][N], double (&r)[K], int gs) {
-  double v[K][N];
-  double cancel = 1.0;
-#pragma unroll
-  for (int i = 0; i < K; i++)
-#pragma unroll
-    for (int j = 0; j < N; j++) v[i][j] = (double)V[i][j];
+CL_HD float renormalise(R (&v)[K][N], R (&r)[K], int gs) {
+  float cancel = 1.0f;
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    double before = 0;
+    R before = 0;
 #pragma unroll
-    for (int j = 0; j < N; j++) before = fma(v[i][j], v[i][j], before);
+    for (int j = 0; j < N; j++) before = vfma(v[i][j], v[i][j], before);
     if (gs == 1) {  // modified
 #pragma unroll
       for (int q = 0; q < i; q++) {
-        double c = 0;
+        R c = 0;
 #pragma unroll
-        for (int j = 0; j < N; j++) c = fma(v[q][j], v[i][j], c);
+        for (int j = 0; j < N; j++) c = vfma(v[q][j], v[i][j], c);
 #pragma unroll
-        for (int j = 0; j < N; j++) v[i][j] = fma(-c, v[q][j], v[i][j]);
+        for (int j = 0; j < N; j++) v[i][j] = vfma(-c, v[q][j], v[i][j]);
       }
     } else {  // classical: all projections against the original v_i
-      double cq[K];
+      R cq[K];
 #pragma unroll
       for (int q = 0; q < i; q++) {
-        double c = 0;
+        R c = 0;
 #pragma unroll
-        for (int j = 0; j < N; j++) c = fma(v[q][j], v[i][j], c);
+        for (int j = 0; j < N; j++) c = vfma(v[q][j], v[i][j], c);
         cq[q] = c;
       }
 #pragma unroll
       for (int q = 0; q < i; q++)
 #pragma unroll
-        for (int j = 0; j < N; j++) v[i][j] = fma(-cq[q], v[q][j], v[i][j]);
+        for (int j = 0; j < N; j++) v[i][j] = vfma(-cq[q], v[q][j], v[i][j]);
     }
-    double s = 0;
+    R s = 0;
 #pragma unroll
-    for (int j = 0; j < N; j++) s = fma(v[i][j], v[i][j], s);
-    const double inv = rsqrt(s);
+    for (int j = 0; j < N; j++) s = vfma(v[i][j], v[i][j], s);
+    const R inv = vrsqrt(s);
     r[i] = s * inv;
-    cancel = fmax(cancel, before * (inv * inv));
+    cancel = fmaxf(cancel, (float)(before * (inv * inv)));
 #pragma unroll
     for (int j = 0; j < N; j++) v[i][j] *= inv;
   }
-#pragma unroll
-  for (int i = 0; i < K; i++)
-#pragma unroll
-    for (int j = 0; j < N; j++) V[i][j] = (R)v[i][j];
   return cancel;
 }
 
@@ -576,9 +594,9 @@ CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
 #pragma unroll
     for (int j = 0; j < N; j++) L.V[i][j] = (i == j) ? R(1) : R(0);
   refresh_tangent_derivs(L);
-  L.fac_old = 1e-4f;
+  L.lfac_old = kLog2FacMin;
   L.t_phase = 0.0;
-  L.t_gs = 0.0;
+  L.t_gs = 0.f;
   if (a.t_align > 0) {
     L.phase = kAlign;
     L.phase_len = a.t_align;
@@ -597,12 +615,12 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
 #pragma unroll
   for (int i = 0; i < N; i++) L.x[i] = (R)a.inits.base[pt * a.inits.ps + i * a.inits.cs];
   L.h = (R)a.h0;
-  L.fac_old = 1e-4f;
+  L.lfac_old = kLog2FacMin;
   L.reject = false;
   L.steps = 0;
   L.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
-  L.L = a.dt_renorm / kRenormSplitInit;
-  L.rate_max = 0.0;
+  L.L = (float)a.dt_renorm / kRenormSplitInit;
+  L.rate_max = 0.f;
 #pragma unroll
   for (int i = 0; i < K; i++) {
     L.sum[i] = L.comp[i] = 0.0;
@@ -619,7 +637,7 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
     L.phase = kTransient;
     L.phase_len = a.t_transient;
     L.t_phase = 0.0;
-    L.t_gs = 0.0;
+    L.t_gs = 0.f;
   } else {
     lane_start_tangent(L, a);
   }
@@ -629,33 +647,36 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
 // phase, interval target adapted.  Returns false on a degenerate basis.
 template <class M, int K, class R, int INTEG>
 CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
-  double r[K];
-  const double cancel = renormalise<M::N, K, R>(L.V, r, a.gs);
+  constexpr R kHuge = sizeof(R) == 4 ? R(3.0e38f) : R(1e300);
+  R r[K];
+  const float cancel = renormalise<M::N, K, R>(L.V, r, a.gs);
   bool ok = true;
 #pragma unroll
-  for (int i = 0; i < K; i++) ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
+  for (int i = 0; i < K; i++) ok = ok && (r[i] > R(0)) && (r[i] < kHuge);
   if (!ok) return false;
   if (L.phase == kAverage) {
-    // Norms multiply into a running product; its log joins the compensated
-    // sum only when it nears the edge of the double range (and at the end),
-    // so most renormalisations take no logarithm at all.
+    // Norms multiply into a running FP64 product; its log joins the
+    // compensated sum only when it nears the edge of the double range (and
+    // at the end), so most renormalisations take no logarithm at all.
     bool flush = false;
 #pragma unroll
     for (int i = 0; i < K; i++) {
-      L.prod[i] *= r[i];
+      L.prod[i] *= (double)r[i];
       flush = flush || !(L.prod[i] < 1e150 && L.prod[i] > 1e-150);
     }
     if (flush) lane_flush_logs(L);
   }
-  if (L.t_gs > 0.0) {  // cancellation per unit time -> next interval
+  if (L.t_gs > 0.f) {  // cancellation per unit time -> next interval
     // The rate varies along an orbit (bursts of strong contraction), so the
-    // interval follows the largest recent rate, forgotten slowly.
-    const double rate = 0.5 * (double)logf((float)cancel) / L.t_gs;
-    L.rate_max = fmax(rate, 0.995 * L.rate_max);
-    const double target = 0.125 * c.tau / fmax(L.rate_max, 1e-30);
-    L.L = fmin(a.dt_renorm, fmax(a.dt_renorm / kRenormSplitMax, target));
+    // interval follows the largest recent rate, forgotten slowly.  These
+    // quantities only steer the interval: single precision, fast division.
+    const float rate = fast_div(0.5f * 0.6931471805599453f * fast_log2f(cancel), L.t_gs);
+    L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
+    const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
+    const float dt = (float)a.dt_renorm;
+    L.L = fminf(dt, fmaxf(dt * (1.0f / kRenormSplitMax), target));
   }
-  L.t_gs = 0.0;
+  L.t_gs = 0.f;
   refresh_tangent_derivs(L);
   return true;
 }
@@ -665,7 +686,7 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
 template <class M, int K, class R, int INTEG>
 CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
   constexpr int N = M::N;
-  constexpr float safe = 0.9f, beta = 0.04f, facc1 = 5.0f, facc2 = 0.1f;
+  constexpr float beta = 0.04f;
   constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
   if (L.steps >= c.max_steps) {
     lane_finish(L, a, 3);
@@ -681,17 +702,21 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
   const bool joint = L.phase != kTransient;
   R x1[N], V1[K][N], kx1[N], kv1[K][N];
   L.steps++;
-  const float err = attempt<M, K, R, INTEG>(L, h, joint, c.rtol, c.atol, x1, V1, kx1, kv1);
-  if (!(err == err) || err > 3.0e38f) {
+  const float err2 = attempt<M, K, R, INTEG>(L, h, joint, c.rtol, c.atol, x1, V1, kx1, kv1);
+  if (!(err2 <= 3.4e38f)) {  // NaN or an overflowed error norm
     lane_finish(L, a, 1);
     return kFinished;
   }
-  const float fac11 = exp2f(expo1 * fast_log2f(fmaxf(err, 1e-30f)));
-  if (err <= 1.0f) {
-    float fac = fac11 * exp2f(-beta * fast_log2f(L.fac_old));
-    fac = fmaxf(facc2, fminf(facc1, fac * (1.0f / safe)));
-    R hnew = h * (R)fast_div(1.0f, fac);
-    L.fac_old = fmaxf(err, 1e-4f);
+  // The controller of dopri.dp.cpp:46-138 in the log2 domain: with
+  // l = log2 err, fac = err^expo1 fac_old^-beta / safe clamped to
+  // [facc2, facc1] = [0.1, 5] becomes lf = expo1 l - beta l_old - log2 safe
+  // clamped to [log2 0.1, log2 5], and h_new = h 2^-lf.
+  const float lerr = 0.5f * fast_log2f(fmaxf(err2, 1e-38f));
+  if (err2 <= 1.0f) {
+    const float lf = fminf(kLog2Facc1, fmaxf(kLog2Facc2, fmaf(expo1, lerr, fmaf(-beta, L.lfac_old,
+                                                                                   -kLog2Safe))));
+    R hnew = h * (R)exp2f(-lf);
+    L.lfac_old = fmaxf(lerr, kLog2FacMin);
 #pragma unroll
     for (int j = 0; j < N; j++) {
       L.x[j] = x1[j];
@@ -711,7 +736,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
     L.reject = false;
     if (!clamped || hnew < h) L.h = hnew;  // else keep the unclamped proposal
     L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
-    L.t_gs += (double)h;
+    L.t_gs += (float)h;
     bool inside = true;
 #pragma unroll
     for (int j = 0; j < N; j++) inside = inside && (fabs(L.x[j]) <= (R)c.escape);
@@ -737,7 +762,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
       }
     }
   } else {
-    L.h = h * (R)fast_div(1.0f, fminf(facc1, fac11 * (1.0f / safe)));
+    L.h = h * (R)exp2f(-fminf(kLog2Facc1, fmaf(expo1, lerr, -kLog2Safe)));
     L.reject = true;
   }
   return kRunning;
