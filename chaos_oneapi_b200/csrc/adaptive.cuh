@@ -15,10 +15,10 @@
 //    arithmetic as one RK step of the joint (n + k n)-dimensional system, with
 //    a register footprint of one vector's stages instead of all of them.
 //  * Renormalisation (see Lane): Gram-Schmidt (classical as
-//    cuda/tools/linalg.dp.cpp:36-51, or modified) in the precision of the
-//    tangent vectors, at intervals of at most dt_renorm (short enough that
-//    little of any vector cancels) and exactly at the phase ends; norms
-//    multiplied and log-norms summed in FP64 with Kahan compensation.
+//    cuda/tools/linalg.dp.cpp:36-51, or modified) in FP64 whatever the state
+//    precision, at intervals of at most dt_renorm and exactly at the phase
+//    ends; norms multiplied and log-norms summed in FP64 with Kahan
+//    compensation.
 #pragma once
 #include <type_traits>
 
@@ -355,12 +355,32 @@ struct Lane {
   double t_phase, phase_len;  // time into the current phase, its length
   float t_gs, L;              // time since the last Gram-Schmidt, its target
   float rate_max;             // largest recent log-cancellation per unit time
-  double t_avg;
-  double sum[K], comp[K];     // Kahan-compensated sums of log-norms
   double prod[K];             // product of the norms since the last log
   int64_t steps;
+};
+
+// The part of a lane's state that a step does not touch -- the compensated
+// log-norm sums (read at the rare flushes of the norm products), the
+// averaging time and the point index (read at phase ends) -- lives in a
+// per-thread slot of shared memory instead of registers, which leaves the
+// registers to the step itself.  Blocks have at most kMaxLaneBlock threads.
+constexpr int kMaxLaneBlock = 128;
+struct Cold {
+  double sum[4], comp[4];  // Kahan-compensated sums of log-norms (k <= 4)
+  double t_avg;
   int64_t pt;
 };
+#ifdef __CUDA_ARCH__
+static __shared__ Cold g_cold[kMaxLaneBlock];
+#endif
+CL_HD Cold &cold_slot() {
+#ifdef __CUDA_ARCH__
+  return g_cold[threadIdx.x];
+#else
+  static thread_local Cold c;  // host form: one lane per thread
+  return c;
+#endif
+}
 
 // Packed FP32 form (odd k): the rows of the joint system -- the state and
 // the k tangent vectors -- advance two at a time as float2 pairs:
@@ -488,20 +508,14 @@ CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol,
   }
 }
 
-// Gram-Schmidt on the k tangent vectors in the precision R of the vectors;
+// Gram-Schmidt in FP64 on the k tangent vectors (whatever their precision R);
 // r[i] = norms after the projections (the R diagonal).  Returns
 // max_i |v_i|^2 / r_i^2: how much of each vector cancelled, i.e. the factor
-// by which errors in the vectors grew relative to what is left of them.
-// Renormalisation keeps that factor near e^(tau / 8), so the projections lose
-// at most a bit or two of R; the log-norms are summed in FP64 by the caller.
-CL_HD float vrsqrt(float s) {
-#ifdef __CUDA_ARCH__
-  return rsqrtf(s);
-#else
-  return 1.0f / sqrtf(s);
-#endif
-}
-CL_HD double vrsqrt(double s) {
+// by which errors in the vectors grew relative to what is left of them (an
+// estimate that only steers the renormalisation interval, so |v_i|^2 before
+// the projections is taken in the vectors' own precision).
+//
+template <class R> CL_HD double rsqrt_for(double s) {
 #ifdef __CUDA_ARCH__
   return rsqrt(s);
 #else
@@ -510,45 +524,55 @@ CL_HD double vrsqrt(double s) {
 }
 
 template <int N, int K, class R>
-CL_HD float renormalise(R (&v)[K][N], R (&r)[K], int gs) {
+CL_HD float renormalise(R (&V)[K][N], double (&r)[K], int gs) {
+  double v[K][N];
   float cancel = 1.0f;
+#pragma unroll
+  for (int i = 0; i < K; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) v[i][j] = (double)V[i][j];
 #pragma unroll
   for (int i = 0; i < K; i++) {
     R before = 0;
 #pragma unroll
-    for (int j = 0; j < N; j++) before = vfma(v[i][j], v[i][j], before);
+    for (int j = 0; j < N; j++) before = vfma(V[i][j], V[i][j], before);
     if (gs == 1) {  // modified
 #pragma unroll
       for (int q = 0; q < i; q++) {
-        R c = 0;
+        double c = 0;
 #pragma unroll
-        for (int j = 0; j < N; j++) c = vfma(v[q][j], v[i][j], c);
+        for (int j = 0; j < N; j++) c = fma(v[q][j], v[i][j], c);
 #pragma unroll
-        for (int j = 0; j < N; j++) v[i][j] = vfma(-c, v[q][j], v[i][j]);
+        for (int j = 0; j < N; j++) v[i][j] = fma(-c, v[q][j], v[i][j]);
       }
     } else {  // classical: all projections against the original v_i
-      R cq[K];
+      double cq[K];
 #pragma unroll
       for (int q = 0; q < i; q++) {
-        R c = 0;
+        double c = 0;
 #pragma unroll
-        for (int j = 0; j < N; j++) c = vfma(v[q][j], v[i][j], c);
+        for (int j = 0; j < N; j++) c = fma(v[q][j], v[i][j], c);
         cq[q] = c;
       }
 #pragma unroll
       for (int q = 0; q < i; q++)
 #pragma unroll
-        for (int j = 0; j < N; j++) v[i][j] = vfma(-cq[q], v[q][j], v[i][j]);
+        for (int j = 0; j < N; j++) v[i][j] = fma(-cq[q], v[q][j], v[i][j]);
     }
-    R s = 0;
+    double s = 0;
 #pragma unroll
-    for (int j = 0; j < N; j++) s = vfma(v[i][j], v[i][j], s);
-    const R inv = vrsqrt(s);
+    for (int j = 0; j < N; j++) s = fma(v[i][j], v[i][j], s);
+    const double inv = rsqrt_for<R>(s);
     r[i] = s * inv;
-    cancel = fmaxf(cancel, (float)(before * (inv * inv)));
+    const float fi = (float)inv;
+    cancel = fmaxf(cancel, (float)before * (fi * fi));
 #pragma unroll
     for (int j = 0; j < N; j++) v[i][j] *= inv;
   }
+#pragma unroll
+  for (int i = 0; i < K; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) V[i][j] = (R)v[i][j];
   return cancel;
 }
 
@@ -565,10 +589,11 @@ template <class M, int K, class R, int INTEG>
 CL_HD void lane_flush_logs(Lane<M, K, R, INTEG> &L) {
 #pragma unroll
   for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
-    const double y = log(L.prod[i]) - L.comp[i];
-    const double s = L.sum[i] + y;
-    L.comp[i] = (s - L.sum[i]) - y;
-    L.sum[i] = s;
+    Cold &c = cold_slot();
+    const double y = log(L.prod[i]) - c.comp[i];
+    const double s = c.sum[i] + y;
+    c.comp[i] = (s - c.sum[i]) - y;
+    c.sum[i] = s;
     L.prod[i] = 1.0;
   }
 }
@@ -576,13 +601,14 @@ CL_HD void lane_flush_logs(Lane<M, K, R, INTEG> &L) {
 template <class M, int K, class R, int INTEG>
 CL_HD void lane_finish(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int status) {
   lane_flush_logs(L);
+  const Cold &c = cold_slot();
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    const double lam = status ? quiet_nan() : L.sum[i] / L.t_avg;
-    a.spectrum.base[L.pt * a.spectrum.ps + i * a.spectrum.cs] = lam;
+    const double lam = status ? quiet_nan() : c.sum[i] / c.t_avg;
+    a.spectrum.base[c.pt * a.spectrum.ps + i * a.spectrum.cs] = lam;
   }
-  if (a.status) a.status[L.pt] = status;
-  if (a.steps) a.steps[L.pt] = L.steps;
+  if (a.status) a.status[c.pt] = status;
+  if (a.steps) a.steps[c.pt] = L.steps;
 }
 
 // Tangent basis = identity, start of the alignment / averaging phases.
@@ -602,14 +628,15 @@ CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
     L.phase_len = a.t_align;
   } else {
     L.phase = kAverage;
-    L.phase_len = L.t_avg;
+    L.phase_len = cold_slot().t_avg;
   }
 }
 
 template <class M, int K, class R, int INTEG>
 CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt) {
   constexpr int N = M::N;
-  L.pt = pt;
+  Cold &cs = cold_slot();
+  cs.pt = pt;
 #pragma unroll
   for (int i = 0; i < M::NP; i++) L.p[i] = (R)a.params.base[pt * a.params.ps + i * a.params.cs];
 #pragma unroll
@@ -618,12 +645,12 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
   L.lfac_old = kLog2FacMin;
   L.reject = false;
   L.steps = 0;
-  L.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
+  cs.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
   L.L = (float)a.dt_renorm / kRenormSplitInit;
   L.rate_max = 0.f;
 #pragma unroll
   for (int i = 0; i < K; i++) {
-    L.sum[i] = L.comp[i] = 0.0;
+    cs.sum[i] = cs.comp[i] = 0.0;
     L.prod[i] = 1.0;
   }
   // The tangent rows ride along in the packed transient pass; start them
@@ -647,12 +674,11 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
 // phase, interval target adapted.  Returns false on a degenerate basis.
 template <class M, int K, class R, int INTEG>
 CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
-  constexpr R kHuge = sizeof(R) == 4 ? R(3.0e38f) : R(1e300);
-  R r[K];
+  double r[K];
   const float cancel = renormalise<M::N, K, R>(L.V, r, a.gs);
   bool ok = true;
 #pragma unroll
-  for (int i = 0; i < K; i++) ok = ok && (r[i] > R(0)) && (r[i] < kHuge);
+  for (int i = 0; i < K; i++) ok = ok && (r[i] > 0.0) && (r[i] < 1e300);
   if (!ok) return false;
   if (L.phase == kAverage) {
     // Norms multiply into a running FP64 product; its log joins the
@@ -661,7 +687,7 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
     bool flush = false;
 #pragma unroll
     for (int i = 0; i < K; i++) {
-      L.prod[i] *= (double)r[i];
+      L.prod[i] *= r[i];
       flush = flush || !(L.prod[i] < 1e150 && L.prod[i] > 1e-150);
     }
     if (flush) lane_flush_logs(L);
@@ -753,7 +779,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
           return kFinished;
         }
         L.phase = kAverage;
-        L.phase_len = L.t_avg;
+        L.phase_len = cold_slot().t_avg;
         L.t_phase = 0.0;
       } else {
         const bool ok = lane_gram_schmidt(L, a, c);
