@@ -346,13 +346,14 @@ def run_batch_bench(a, rank, world, local):
         clk = clocks.stop()
         elapsed_ms = t0e.elapsed_time(t1e)
         # the same work without batching: three direct launches in a row
-        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        d0.record(stream)
-        for sw_d, pt in zip(direct, parts):
+        dev_ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(parts) + 1)]
+        dev_ev[0].record(stream)
+        for i, (sw_d, pt) in enumerate(zip(direct, parts)):
             sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
-        d1.record(stream)
+            dev_ev[i + 1].record(stream)
         stream.synchronize()
-        direct_ms = d0.elapsed_time(d1)
+        direct_ms = dev_ev[0].elapsed_time(dev_ev[-1])
+        direct_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
         # end to end: inputs from pinned host memory, results back, each step
         torch.cuda.synchronize(dev)
         e0 = time.perf_counter()
@@ -376,7 +377,9 @@ def run_batch_bench(a, rank, world, local):
         stt = st.cpu().numpy()
         fl += float(stp.sum()) * flops_per_step(sw.cfg.model, "dopri5")
         pts[sw.cfg.model] = {"points": int(p.shape[0]), "ok": int((stt == 0).sum()),
-                             "escaped": int((stt == 4).sum()), "steps_mean": float(stp.mean())}
+                             "escaped": int((stt == 4).sum()), "steps_mean": float(stp.mean()),
+                             "steps_p99": float(np.percentile(stp, 99)),
+                             "steps_max": int(stp.max())}
     achieved = fl / (elapsed_ms / a.steps * 1e-3) / 1e12
     h2d = sum(int(h.numel() * 8) for hs in host for h in hs)
     d2h = sum(int(o[0].numel() * 8 + o[1].numel() * 4) for o in outs)
@@ -396,6 +399,7 @@ def run_batch_bench(a, rank, world, local):
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-process (FMA-chain kernel)"},
             "unbatched": {"ms": direct_ms, "points_per_s": total_points / (direct_ms * 1e-3),
+                          "segment_ms": direct_seg_ms,
                           "how": "the three sweeps launched in turn, one thread per point, "
                                  "no work queue"},
             "e2e": {"value": total_points * world / e2e_s, "unit": "points/s",

@@ -39,6 +39,7 @@ CUDA_UNITS = {
     "capi.cu": [],
     "peak.cu": [],
     "static_scratch.cu": [],
+    "order.cu": [],
     "mlp.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]

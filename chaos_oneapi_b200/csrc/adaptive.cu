@@ -17,9 +17,12 @@ namespace adaptive {
 // coprime to P, so a permutation): neighbouring grid points cost alike, and
 // spreading them over the run keeps a cluster of expensive points (a chaotic
 // band, escaping orbits) from forming the tail of the launch.
+// With an explicit order (longest averaging time first, order.cu) the queue
+// hands out order[q] instead.
 __device__ __forceinline__ int64_t next_point(const AdaptiveArgs &a) {
   const unsigned long long q = atomicAdd(a.queue, 1ULL);
   if (q >= (unsigned long long)a.P) return a.P;
+  if (a.order) return (int64_t)a.order[q];
   return (int64_t)((q * (unsigned long long)a.queue_stride) % (unsigned long long)a.P);
 }
 
@@ -134,7 +137,9 @@ __device__ __forceinline__ bool batch_take(const BatchArgs &b, int seg, int64_t 
   const int64_t P = b.seg[seg].P;
   const unsigned long long q = atomicAdd(&b.queues[seg], 1ULL);
   if (q >= (unsigned long long)P) return false;
-  pt = (int64_t)((q * (unsigned long long)b.seg[seg].queue_stride) % (unsigned long long)P);
+  pt = b.seg[seg].order
+           ? (int64_t)b.seg[seg].order[q]
+           : (int64_t)((q * (unsigned long long)b.seg[seg].queue_stride) % (unsigned long long)P);
   return true;
 }
 

@@ -382,14 +382,17 @@ CL_HD Cold &cold_slot() {
 #endif
 }
 
-// Packed FP32 form (odd k): the rows of the joint system -- the state and
-// the k tangent vectors -- advance two at a time as float2 pairs:
+// Packed FP32 form: the rows of the joint system -- the state and the k
+// tangent vectors -- advance two at a time as float2 pairs.  Odd k:
 // (state, v_{k-1}) in one pass, which also records the stage points, then
-// (v_0, v_1), (v_2, v_3), ... at those stage points.  Each stage combination
-// of two rows is then one packed multiply-add per coefficient instead of two.
+// (v_0, v_1), (v_2, v_3), ... at those stage points.  Even k: the state alone
+// (recording the stage points), then the same vector pairs.  Each stage
+// combination of two rows is then one packed multiply-add per coefficient
+// instead of two.
 template <class M, int K, class R>
 struct Packed {
-  static constexpr bool value = std::is_same<R, float>::value && (K % 2 == 1);
+  static constexpr bool value = std::is_same<R, float>::value && K >= 2;
+  static constexpr bool state_paired = (K % 2 == 1);
 };
 
 template <class M>
@@ -445,31 +448,39 @@ CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol,
   const float inv_nc = joint ? 1.0f / (N * (1 + K)) : 1.0f / N;
   R X[S][N];
   if constexpr (Packed<M, K, R>::value) {
-    float2 ya[N], ka[N], ya1[N], ka1[N];
-#pragma unroll
-    for (int j = 0; j < N; j++) {
-      ya[j] = make_float2(st.x[j], st.V[K - 1][j]);
-      ka[j] = make_float2(st.kx[j], st.kv[K - 1][j]);
-    }
+    constexpr bool SP = Packed<M, K, R>::state_paired;
+    constexpr int KV = SP ? K - 1 : K;  // vectors advanced in pairs (v_0 .. v_{KV-1})
     float2 ea = make_float2(0.f, 0.f);
-    PairStateStages<M> fa{st.p, X};
-    if (INTEG == kDverk65) dverk_pass<N, float2>(ya, h, fa, ya1, ea, rtol, atol);
-    else dopri_pass<N, float2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+    if constexpr (SP) {
+      float2 ya[N], ka[N], ya1[N], ka1[N];
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-      x1[j] = ya1[j].x;
-      V1[K - 1][j] = ya1[j].y;
-      if (INTEG == kDopri5) {
-        kx1[j] = ka1[j].x;
-        kv1[K - 1][j] = ka1[j].y;
+      for (int j = 0; j < N; j++) {
+        ya[j] = make_float2(st.x[j], st.V[K - 1][j]);
+        ka[j] = make_float2(st.kx[j], st.kv[K - 1][j]);
       }
+      PairStateStages<M> fa{st.p, X};
+      if (INTEG == kDverk65) dverk_pass<N, float2>(ya, h, fa, ya1, ea, rtol, atol);
+      else dopri_pass<N, float2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        x1[j] = ya1[j].x;
+        V1[K - 1][j] = ya1[j].y;
+        if (INTEG == kDopri5) {
+          kx1[j] = ka1[j].x;
+          kv1[K - 1][j] = ka1[j].y;
+        }
+      }
+    } else {
+      StateStages<M, R> fs{st.p, X};
+      if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, ea.x, rtol, atol);
+      else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, ea.x, rtol, atol);
     }
     float err2 = ea.x;
     if (joint) {
       float2 eb = make_float2(0.f, 0.f);
       PairTangentStages<M> fb{st.p, st.x, X};
 #pragma unroll
-      for (int m = 0; m + 1 < K; m += 2) {
+      for (int m = 0; m + 1 < KV; m += 2) {
         float2 yb[N], kb[N], yb1[N], kb1[N];
 #pragma unroll
         for (int j = 0; j < N; j++) {

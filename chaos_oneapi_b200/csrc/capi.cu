@@ -109,6 +109,10 @@ struct chaos_lyap_handle {
   cudaStream_t own_stream = nullptr;
   cudaStream_t last_stream = nullptr;
   unsigned long long *queue = nullptr;  // point counters: persistent sweep / batch segments
+  // longest-first hand-out order of points with their own averaging times
+  int32_t *order = nullptr;
+  void *order_scratch = nullptr;
+  int64_t order_cap = 0;
   // host-path staging
   double *s_params = nullptr, *s_inits = nullptr, *s_spec = nullptr, *s_tavg = nullptr;
   int32_t *s_status = nullptr;
@@ -271,8 +275,29 @@ int chaos_lyap_destroy(chaos_lyap_handle *h) {
   cudaStreamSynchronize(h->own_stream);
   free_staging(h);
   cudaFree(h->queue);
+  cudaFree(h->order);
+  cudaFree(h->order_scratch);
   cudaStreamDestroy(h->own_stream);
   delete h;
+  return CHAOS_LYAP_OK;
+}
+
+// Device buffers for the longest-first order of P points (grown on demand;
+// allocated outside any stream capture: before a run or a graph capture).
+static int ensure_order(chaos_lyap_handle *h, int64_t P) {
+  if (P <= h->order_cap) return CHAOS_LYAP_OK;
+  DeviceGuard g(h->d.device);
+  cudaFree(h->order);
+  h->order = nullptr;
+  h->order_cap = 0;
+  cudaError_t e = cudaMalloc(&h->order, sizeof(int32_t) * P);
+  if (e == cudaSuccess && !h->order_scratch) e = cudaMalloc(&h->order_scratch, chaos::kOrderScratchBytes);
+  if (e != cudaSuccess) {
+    cudaFree(h->order);
+    h->order = nullptr;
+    return fail(CHAOS_LYAP_ENOMEM, "cudaMalloc(order): %s", cudaGetErrorString(e));
+  }
+  h->order_cap = P;
   return CHAOS_LYAP_OK;
 }
 
@@ -330,6 +355,12 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
       if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
       a.queue = h->queue;
       a.queue_stride = chaos::queue_stride_for(P);
+      if (a.t_avg_per_point && m->dim <= 4) {  // longest averaging time first
+        if ((rc = ensure_order(h, P))) return rc;
+        rc = chaos::launch_order_longest_first(a.t_avg_per_point, P, h->order, h->order_scratch, s);
+        if (rc) return cuda_fail((cudaError_t)rc, "order launch");
+        a.order = h->order;
+      }
     }
     if (m->dim > 4) rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
     else rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
@@ -519,6 +550,12 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArg
     a.status = sg.status;
     a.steps = sg.steps;
     a.queue_stride = chaos::queue_stride_for(sg.P);
+    a.order = nullptr;
+    if (sg.t_avg_per_point && sg.P > 0) {  // longest averaging time first
+      int rc = ensure_order(sg.handle, sg.P);
+      if (rc) return rc;
+      a.order = sg.handle->order;
+    }
     b->model[i] = m->id;
   }
   b->queues = segs[0].handle->queue;
@@ -529,10 +566,18 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArg
   return CHAOS_LYAP_OK;
 }
 
-static int enqueue_batch(const chaos::BatchArgs &b, int integ, int prec, int block, cudaStream_t s) {
+static int enqueue_batch(const chaos::BatchArgs &b, const chaos_lyap_segment *segs, int integ,
+                         int prec, int block, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(b.queues, 0, sizeof(unsigned long long) * b.nseg, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
-  int rc = chaos::launch_batch(integ, prec, b, block, s);
+  int rc;
+  for (int i = 0; i < b.nseg; i++) {
+    if (!b.seg[i].order) continue;
+    rc = chaos::launch_order_longest_first(b.seg[i].t_avg_per_point, b.seg[i].P,
+                                           segs[i].handle->order, segs[i].handle->order_scratch, s);
+    if (rc) return cuda_fail((cudaError_t)rc, "order launch");
+  }
+  rc = chaos::launch_batch(integ, prec, b, block, s);
   if (rc == chaos::kErrUnsupported) return fail(CHAOS_LYAP_EUNSUPPORTED, "no batch kernel for this mix");
   if (rc) return cuda_fail((cudaError_t)rc, "batch launch");
   return CHAOS_LYAP_OK;
@@ -544,7 +589,7 @@ int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream)
   int rc = build_batch(segs, nseg, &b, &integ, &prec, &block);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
-  rc = enqueue_batch(b, integ, prec, block, (cudaStream_t)stream);
+  rc = enqueue_batch(b, segs, integ, prec, block, (cudaStream_t)stream);
   if (!rc) segs[0].handle->last_stream = (cudaStream_t)stream;
   return rc;
 }
@@ -570,7 +615,7 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
   gr->device = segs[0].handle->d.device;
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rc = enqueue_batch(b, integ, prec, block, cs);
+    rc = enqueue_batch(b, segs, integ, prec, block, cs);
     cudaError_t e2 = cudaStreamEndCapture(cs, &gr->graph);
     if (!rc && e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
   } else {

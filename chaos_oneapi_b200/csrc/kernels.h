@@ -51,7 +51,15 @@ struct AdaptiveArgs {
   // persistent work-queue form
   unsigned long long *queue;  // nullable unless the launch is persistent
   uint64_t queue_stride;      // coprime to P: hand-out order q -> q * stride mod P
+  const int32_t *order;       // nullable: hand-out order q -> order[q] (overrides the stride)
 };
+
+// Longest-first hand-out order (order.cu): order = a permutation of [0, P)
+// by decreasing t_avg (bucketed); scratch holds kOrderScratchBytes.
+constexpr int kOrderBuckets = 1024;
+constexpr size_t kOrderScratchBytes = 2 * sizeof(unsigned long long) + kOrderBuckets * sizeof(unsigned int);
+int launch_order_longest_first(const double *t_avg, int64_t P, int32_t *order, void *scratch,
+                               cudaStream_t s);
 
 // A stride for the persistent queue's permutation: a prime that does not
 // divide P (so q -> q * stride mod P is a bijection on [0, P)).

@@ -43,6 +43,9 @@ def _single(lib, part, torch):
 
 def _check(parts, results, singles):
     for (sw, p, _, _, _, _, _), (spec, st), (s1, st1) in zip(parts, results, singles):
+        # every point handed out exactly once (the longest-first order is a
+        # permutation): no status left at its -1 fill
+        assert (st >= 0).all() and (st1 >= 0).all()
         assert (st == st1).mean() > 0.95
         ok = (st == 0) & (st1 == 0)
         assert ok.mean() > 0.5  # hyper-Rossler leaves every bounded set for part of its range
