@@ -304,15 +304,17 @@ def run_batch_bench(a, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     rng = np.random.default_rng(100 + rank)
-    parts, host, sweeps, direct = [], [], [], []
+    parts, host, sweeps, direct, direct_split = [], [], [], [], []
+    form = "split_persistent" if a.batch_form == "split" else "persistent"
     for name, seg in BATCH.items():
         params = cl.make_grid(len(seg["base"]), seg["base"], seg["s1"], seg["s2"])
         P = params.shape[0]
         inits = cl.make_inits(len(seg["x0"]), P, seg["x0"], 1e-3, "uniform", rank)
         tavg = rng.uniform(1000.0, 10000.0, P)
-        sw = cl.Sweep(model=name, device=local, schedule="persistent", **BATCH_KW)
+        sw = cl.Sweep(model=name, device=local, schedule=form, **BATCH_KW)
         sweeps.append(sw)
         direct.append(cl.Sweep(model=name, device=local, schedule="direct", **BATCH_KW))
+        direct_split.append(cl.Sweep(model=name, device=local, schedule="split", **BATCH_KW))
         k = sw.k
         bufs = [torch.from_numpy(x).to(dev) for x in (params, inits, tavg)]
         spec = torch.empty((P, k), dtype=torch.float64, device=dev)
@@ -354,6 +356,14 @@ def run_batch_bench(a, rank, world, local):
         stream.synchronize()
         direct_ms = dev_ev[0].elapsed_time(dev_ev[-1])
         direct_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
+        # and the same three sweeps in the split form (four lanes per point)
+        dev_ev[0].record(stream)
+        for i, (sw_d, pt) in enumerate(zip(direct_split, parts)):
+            sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
+            dev_ev[i + 1].record(stream)
+        stream.synchronize()
+        split_ms = dev_ev[0].elapsed_time(dev_ev[-1])
+        split_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
         # end to end: inputs from pinned host memory, results back, each step
         torch.cuda.synchronize(dev)
         e0 = time.perf_counter()
@@ -393,15 +403,18 @@ def run_batch_bench(a, rank, world, local):
             "config": {"workload": "batch256", "segments": list(BATCH),
                        "points_per_step": total_points, "t_avg": "U[1000, 10000] per point",
                        **{k: v for k, v in BATCH_KW.items() if k != "t_avg"},
-                       "launch": "one persistent batch kernel per step, replayed CUDA graph"},
+                       "launch": "one persistent batch kernel per step, replayed CUDA graph",
+                       "form": ("one point per group of four lanes" if a.batch_form == "split"
+                                else "one point per lane")},
             "gpu_launches": a.steps, "clocks": clk,
             "roofline": {"bound": "fp32_fma", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-process (FMA-chain kernel)"},
             "unbatched": {"ms": direct_ms, "points_per_s": total_points / (direct_ms * 1e-3),
                           "segment_ms": direct_seg_ms,
-                          "how": "the three sweeps launched in turn, one thread per point, "
-                                 "no work queue"},
+                          "split_ms": split_ms, "split_segment_ms": split_seg_ms,
+                          "how": "the three sweeps launched in turn, no work queue: ms one "
+                                 "thread per point, split_ms one group of four lanes per point"},
             "e2e": {"value": total_points * world / e2e_s, "unit": "points/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": 1},
             "points": pts,
@@ -431,6 +444,8 @@ def main():
     ap.add_argument("--workload", default="rossler1024",
                     choices=sorted(WORKLOADS) + ["batch256", "surrogate"])
     ap.add_argument("--map-size", type=int, default=4096, help="surrogate workload: cells per side")
+    ap.add_argument("--batch-form", default="split", choices=["split", "lane"],
+                    help="batch256: one point per group of four lanes, or per lane")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-sample", type=int, default=256)
     ap.add_argument("--variant", type=int, default=-1,

@@ -40,6 +40,7 @@ CUDA_UNITS = {
     "peak.cu": [],
     "static_scratch.cu": [],
     "order.cu": [],
+    "split.cu": [],
     "mlp.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]

@@ -241,7 +241,9 @@ int chaos_lyap_create(const chaos_lyap_desc *desc, chaos_lyap_handle **out) {
   h->model = m;
   cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, d.device);
   h->block = d.block > 0 ? d.block : (d.precision == CHAOS_PREC_COMPAT_FP64 ? 64 : 128);
-  h->schedule = d.schedule == CHAOS_SCHED_DIRECT ? CHAOS_SCHED_DIRECT : CHAOS_SCHED_PERSISTENT;
+  h->schedule = (d.schedule >= CHAOS_SCHED_DIRECT && d.schedule <= CHAOS_SCHED_SPLIT_PERSISTENT)
+                    ? d.schedule
+                    : CHAOS_SCHED_PERSISTENT;
   h->variant = d.variant == 1 ? 1 : 0;
   if ((e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking)) != cudaSuccess) {
     delete h;
@@ -350,7 +352,8 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
     a.steps = steps;
     const int integ = d.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
     const int prec = d.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
-    if (schedule == CHAOS_SCHED_PERSISTENT) {
+    const bool split = schedule == CHAOS_SCHED_SPLIT_DIRECT || schedule == CHAOS_SCHED_SPLIT_PERSISTENT;
+    if (schedule == CHAOS_SCHED_PERSISTENT || schedule == CHAOS_SCHED_SPLIT_PERSISTENT) {
       cudaError_t e = cudaMemsetAsync(h->queue, 0, sizeof(unsigned long long), s);
       if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queue)");
       a.queue = h->queue;
@@ -363,6 +366,7 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
       }
     }
     if (m->dim > 4) rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
+    else if (split) rc = chaos::launch_split(m->id, integ, prec, a, block, s);
     else rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
   }
   if (rc == chaos::kErrUnsupported)
@@ -471,7 +475,8 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   const int blocks[] = {64, 128};
-  const int scheds[] = {CHAOS_SCHED_DIRECT, CHAOS_SCHED_PERSISTENT};
+  const int scheds[] = {CHAOS_SCHED_DIRECT, CHAOS_SCHED_PERSISTENT, CHAOS_SCHED_SPLIT_DIRECT,
+                        CHAOS_SCHED_SPLIT_PERSISTENT};
   const int nvar = h->d.precision == CHAOS_PREC_FP32 ? 2 : 1;
   float best = 1e30f;
   int best_b = h->block, best_s = h->schedule, best_v = h->variant, rc = CHAOS_LYAP_OK;
@@ -479,6 +484,8 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   for (int v = 0; v < nvar && rc == CHAOS_LYAP_OK; v++)
     for (int b : blocks)
       for (int sc : scheds) {
+        // the register-cap variants exist for the one-lane forms only
+        if (v > 0 && (sc == CHAOS_SCHED_SPLIT_DIRECT || sc == CHAOS_SCHED_SPLIT_PERSISTENT)) continue;
         float ms = 0;
         for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
           cudaEventRecord(e0, s);
@@ -509,7 +516,7 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
 }
 
 static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArgs *b,
-                       int *integ, int *prec, int *block) {
+                       int *integ, int *prec, int *block, bool *split) {
   if (!segs || nseg <= 0 || nseg > chaos::kMaxSegments)
     return fail(CHAOS_LYAP_EINVAL, "nseg must be 1..%d", chaos::kMaxSegments);
   std::memset(b, 0, sizeof *b);
@@ -563,11 +570,13 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArg
   *integ = d0.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
   *prec = d0.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
   *block = segs[0].handle->block;
+  *split = segs[0].handle->schedule == CHAOS_SCHED_SPLIT_DIRECT ||
+           segs[0].handle->schedule == CHAOS_SCHED_SPLIT_PERSISTENT;
   return CHAOS_LYAP_OK;
 }
 
 static int enqueue_batch(const chaos::BatchArgs &b, const chaos_lyap_segment *segs, int integ,
-                         int prec, int block, cudaStream_t s) {
+                         int prec, int block, bool split, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(b.queues, 0, sizeof(unsigned long long) * b.nseg, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
   int rc;
@@ -577,7 +586,8 @@ static int enqueue_batch(const chaos::BatchArgs &b, const chaos_lyap_segment *se
                                            segs[i].handle->order, segs[i].handle->order_scratch, s);
     if (rc) return cuda_fail((cudaError_t)rc, "order launch");
   }
-  rc = chaos::launch_batch(integ, prec, b, block, s);
+  rc = split ? chaos::launch_batch_split(integ, prec, b, block, s)
+             : chaos::launch_batch(integ, prec, b, block, s);
   if (rc == chaos::kErrUnsupported) return fail(CHAOS_LYAP_EUNSUPPORTED, "no batch kernel for this mix");
   if (rc) return cuda_fail((cudaError_t)rc, "batch launch");
   return CHAOS_LYAP_OK;
@@ -586,10 +596,11 @@ static int enqueue_batch(const chaos::BatchArgs &b, const chaos_lyap_segment *se
 int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream) {
   chaos::BatchArgs b;
   int integ, prec, block;
-  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block);
+  bool split;
+  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block, &split);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
-  rc = enqueue_batch(b, segs, integ, prec, block, (cudaStream_t)stream);
+  rc = enqueue_batch(b, segs, integ, prec, block, split, (cudaStream_t)stream);
   if (!rc) segs[0].handle->last_stream = (cudaStream_t)stream;
   return rc;
 }
@@ -605,7 +616,8 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
   *out = nullptr;
   chaos::BatchArgs b;
   int integ, prec, block;
-  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block);
+  bool split;
+  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block, &split);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
   cudaStream_t cs;
@@ -615,7 +627,7 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
   gr->device = segs[0].handle->d.device;
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rc = enqueue_batch(b, segs, integ, prec, block, cs);
+    rc = enqueue_batch(b, segs, integ, prec, block, split, cs);
     cudaError_t e2 = cudaStreamEndCapture(cs, &gr->graph);
     if (!rc && e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
   } else {

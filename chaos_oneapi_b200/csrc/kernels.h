@@ -102,6 +102,12 @@ struct BatchArgs {
 
 int launch_batch(int integrator, int precision, const BatchArgs &b, int block, cudaStream_t s);
 
+// Split form (split.cu): one point per group of four lanes.
+int launch_split(int model, int integrator, int precision, const AdaptiveArgs &a, int block,
+                 cudaStream_t s);
+int launch_batch_split(int integrator, int precision, const BatchArgs &b, int block,
+                       cudaStream_t s);
+
 }  // namespace chaos
 
 namespace chaos {

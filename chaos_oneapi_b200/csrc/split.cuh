@@ -1,0 +1,352 @@
+// Split form of the adaptive integrator: one parameter point per group of
+// kSplitLanes = 4 consecutive lanes of a warp.  Lane r of a group carries the
+// state and tangent vector v_r (rows r >= k carry none).
+//
+// Why: with one lane per point a step is a serial chain of passes over the
+// state and all k vectors, so a point's time is its step count times that
+// chain.  That bounds a sweep whose points are few (a 64 x 64 map fills a
+// tenth of the GPU) or whose run is set by its longest point (a batch with
+// per-point averaging times: one stiff point with 10^7 steps).  Split over a
+// group, each lane advances only the state and one vector per step (in FP32
+// one packed pair pass), so a step's chain is about half as long, at the
+// price of computing the state in every lane of the group.
+//
+// Consistency: every lane of a group computes the state with the same
+// operations on the same inputs, so the state, the step size, every accept /
+// reject decision and every phase change agree bit for bit across the
+// group.  The two quantities that combine the lanes -- the error norm (a sum)
+// and the Gram-Schmidt cancellation estimate (a max) -- are butterfly
+// reductions (__shfl_xor_sync 1, 2), whose result is the same in all four
+// lanes because IEEE addition and max are commutative.  Gram-Schmidt runs in
+// k rounds: lane q normalises its vector (all projections on earlier vectors
+// already subtracted) and broadcasts it; lanes r > q subtract their
+// projection on it, with the coefficient taken against the original vector
+// (classical, cuda/tools/linalg.dp.cpp:36-51) or the updated one (modified):
+// the same FP64 operations in the same order as the one-lane form.
+#pragma once
+#include "adaptive.cuh"
+
+namespace chaos {
+namespace adaptive {
+
+constexpr int kSplitLanes = 4;
+
+struct Group {
+  int r;          // this lane's row (tangent vector index)
+  int base;       // lane index of the group's first lane
+  unsigned mask;  // the group's four lanes
+};
+__device__ __forceinline__ Group group_of() {
+  const int lane = (int)(threadIdx.x & 31);
+  return Group{lane & 3, lane & ~3, 0xFu << (lane & ~3)};
+}
+
+__device__ __forceinline__ float group_sum(float e, unsigned mask) {
+  e += __shfl_xor_sync(mask, e, 1);
+  e += __shfl_xor_sync(mask, e, 2);
+  return e;
+}
+__device__ __forceinline__ float group_max(float e, unsigned mask) {
+  e = fmaxf(e, __shfl_xor_sync(mask, e, 1));
+  e = fmaxf(e, __shfl_xor_sync(mask, e, 2));
+  return e;
+}
+
+template <class M, class R, int INTEG>
+struct SplitLane {
+  static constexpr int N = M::N;
+  R p[M::NP];
+  R x[N];         // the state (the same in all lanes of the group)
+  R v[N];         // this lane's tangent vector (zero for rows >= k)
+  R kx[N], kv[N]; // Dopri5 FSAL derivatives
+  R h;
+  float lfac_old;
+  int32_t phase;
+  bool reject;
+  double t_phase, phase_len;
+  float t_gs, L, rate_max;
+  double prod;    // product of this vector's norms since the last log
+  int64_t steps;
+};
+
+template <class M, class R, int INTEG>
+__device__ __forceinline__ void split_flush(SplitLane<M, R, INTEG> &L) {
+  Cold &c = cold_slot();
+  const double y = log(L.prod) - c.comp[0];
+  const double s = c.sum[0] + y;
+  c.comp[0] = (s - c.sum[0]) - y;
+  c.sum[0] = s;
+  L.prod = 1.0;
+}
+
+template <class M, class R, int INTEG>
+__device__ void split_finish(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Group &g,
+                             int status) {
+  const Cold &c = cold_slot();
+  if (g.r < a.k) {
+    split_flush(L);
+    const double lam = status ? quiet_nan() : c.sum[0] / c.t_avg;
+    a.spectrum.base[c.pt * a.spectrum.ps + g.r * a.spectrum.cs] = lam;
+  }
+  if (g.r == 0) {
+    if (a.status) a.status[c.pt] = status;
+    if (a.steps) a.steps[c.pt] = L.steps;
+  }
+}
+
+template <class M, class R, int INTEG>
+__device__ void split_start_tangent(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a,
+                                    const Group &g) {
+  constexpr int N = M::N;
+#pragma unroll
+  for (int j = 0; j < N; j++) L.v[j] = (j == g.r && g.r < a.k) ? R(1) : R(0);
+  if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
+  L.lfac_old = kLog2FacMin;
+  L.t_phase = 0.0;
+  L.t_gs = 0.f;
+  if (a.t_align > 0) {
+    L.phase = kAlign;
+    L.phase_len = a.t_align;
+  } else {
+    L.phase = kAverage;
+    L.phase_len = cold_slot().t_avg;
+  }
+}
+
+template <class M, class R, int INTEG>
+__device__ void split_start(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt,
+                            const Group &g) {
+  constexpr int N = M::N;
+  Cold &cs = cold_slot();
+  cs.pt = pt;
+  cs.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
+  cs.sum[0] = cs.comp[0] = 0.0;
+#pragma unroll
+  for (int i = 0; i < M::NP; i++) L.p[i] = (R)a.params.base[pt * a.params.ps + i * a.params.cs];
+#pragma unroll
+  for (int i = 0; i < N; i++) L.x[i] = (R)a.inits.base[pt * a.inits.ps + i * a.inits.cs];
+#pragma unroll
+  for (int j = 0; j < N; j++) L.v[j] = L.kv[j] = R(0);
+  L.h = (R)a.h0;
+  L.lfac_old = kLog2FacMin;
+  L.reject = false;
+  L.steps = 0;
+  L.L = (float)a.dt_renorm / kRenormSplitInit;
+  L.rate_max = 0.f;
+  L.prod = 1.0;
+  if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
+  if (a.t_transient > 0) {
+    L.phase = kTransient;
+    L.phase_len = a.t_transient;
+    L.t_phase = 0.0;
+    L.t_gs = 0.f;
+  } else {
+    split_start_tangent(L, a, g);
+  }
+}
+
+// One step attempt: the state and this lane's vector; returns the group's
+// mean square weighted error (the same in all four lanes).
+template <class M, class R, int INTEG>
+__device__ float split_attempt(const SplitLane<M, R, INTEG> &st, R h, bool joint, bool has_vec,
+                               const Group &g, float rtol, float atol, R (&x1)[M::N],
+                               R (&v1)[M::N], R (&kx1)[M::N], R (&kv1)[M::N]) {
+  constexpr int N = M::N;
+  constexpr int S = (INTEG == kDverk65) ? 8 : 7;
+  float es = 0.f, ev = 0.f;
+  if constexpr (std::is_same<R, float>::value) {  // (state, v_r) as one packed pass
+    float X[S][N];
+    float2 ya[N], ka[N], ya1[N], ka1[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      ya[j] = make_float2(st.x[j], st.v[j]);
+      ka[j] = make_float2(st.kx[j], st.kv[j]);
+    }
+    float2 ea = make_float2(0.f, 0.f);
+    PairStateStages<M> fa{st.p, X};
+    if (INTEG == kDverk65) dverk_pass<N, float2>(ya, h, fa, ya1, ea, rtol, atol);
+    else dopri_pass<N, float2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      x1[j] = ya1[j].x;
+      v1[j] = ya1[j].y;
+      if (INTEG == kDopri5) {
+        kx1[j] = ka1[j].x;
+        kv1[j] = ka1[j].y;
+      }
+    }
+    es = ea.x;
+    ev = ea.y;
+  } else {
+    R X[S][N];
+    StateStages<M, R> fs{st.p, X};
+    if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, es, rtol, atol);
+    else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, es, rtol, atol);
+    if (joint) {
+      TangentStages<M, R> ft{st.p, st.x, X};
+      if (INTEG == kDverk65) dverk_pass<N, R>(st.v, h, ft, v1, ev, rtol, atol);
+      else dopri_pass<N, R>(st.v, st.kv, h, ft, v1, kv1, ev, rtol, atol);
+    }
+  }
+  // the state's error once (lane 0), each vector's in its own lane
+  float e = (g.r == 0 ? es : 0.f) + ((joint && has_vec) ? ev : 0.f);
+  e = group_sum(e, g.mask);
+  const float inv_nc = joint ? 1.0f / (N * (1 + M::N)) : 1.0f / N;
+  return e * inv_nc;
+}
+
+// Gram-Schmidt over the group in FP64 (see the header); false on a
+// degenerate basis (the same answer in all four lanes).
+template <class M, class R, int INTEG>
+__device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a,
+                                   const Ctl &c, const Group &g) {
+  constexpr int N = M::N;
+  const int k = a.k;
+  const bool has_vec = g.r < k;
+  double vo[N], w[N];
+  R before = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    vo[j] = (double)L.v[j];
+    w[j] = vo[j];
+    before = vfma(L.v[j], L.v[j], before);
+  }
+  double rr = 1.0;
+  float cancel = 1.0f;
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+    if (q >= k) break;  // k is the same in all lanes
+    if (g.r == q) {
+      double s = 0;
+#pragma unroll
+      for (int j = 0; j < N; j++) s = fma(w[j], w[j], s);
+      const double inv = rsqrt_for<R>(s);
+      rr = s * inv;
+      const float fi = (float)inv;
+      cancel = fmaxf(cancel, (float)before * (fi * fi));
+#pragma unroll
+      for (int j = 0; j < N; j++) w[j] *= inv;
+    }
+    double qv[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) qv[j] = __shfl_sync(g.mask, w[j], g.base + q);
+    if (g.r > q) {
+      double cq = 0;
+      if (a.gs == 1) {  // modified: against the updated vector
+#pragma unroll
+        for (int j = 0; j < N; j++) cq = fma(qv[j], w[j], cq);
+      } else {  // classical: against the original vector
+#pragma unroll
+        for (int j = 0; j < N; j++) cq = fma(qv[j], vo[j], cq);
+      }
+#pragma unroll
+      for (int j = 0; j < N; j++) w[j] = fma(-cq, qv[j], w[j]);
+    }
+  }
+  const bool ok_own = !has_vec || ((rr > 0.0) && (rr < 1e300));
+  if (!__all_sync(g.mask, ok_own)) return false;
+#pragma unroll
+  for (int j = 0; j < N; j++) L.v[j] = has_vec ? (R)w[j] : R(0);
+  cancel = group_max(cancel, g.mask);
+  if (L.phase == kAverage && has_vec) {
+    L.prod *= rr;
+    if (!(L.prod < 1e150 && L.prod > 1e-150)) split_flush(L);
+  }
+  if (L.t_gs > 0.f) {  // the interval rule of the one-lane form, on the group's max
+    const float rate = fast_div(0.5f * 0.6931471805599453f * fast_log2f(cancel), L.t_gs);
+    L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
+    const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
+    const float dt = (float)a.dt_renorm;
+    L.L = fminf(dt, fmaxf(dt * (1.0f / kRenormSplitMax), target));
+  }
+  L.t_gs = 0.f;
+  if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
+  return true;
+}
+
+// One step attempt of the group, phase bookkeeping included (the one-lane
+// form's lane_step, with the group's error norm and Gram-Schmidt).
+template <class M, class R, int INTEG>
+__device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c,
+                          const Group &g) {
+  constexpr int N = M::N;
+  constexpr float beta = 0.04f;
+  constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
+  if (L.steps >= c.max_steps) {
+    split_finish(L, a, g, 3);
+    return kFinished;
+  }
+  if (!((double)L.h >= c.hmin)) {
+    split_finish(L, a, g, 2);
+    return kFinished;
+  }
+  const double remaining = L.phase_len - L.t_phase;
+  const bool clamped = (double)L.h >= remaining;
+  const R h = clamped ? (R)remaining : L.h;
+  const bool joint = L.phase != kTransient;
+  const bool has_vec = g.r < a.k;
+  R x1[N], v1[N], kx1[N], kv1[N];
+  L.steps++;
+  const float err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, c.rtol, c.atol, x1, v1,
+                                                kx1, kv1);
+  if (!(err2 <= 3.4e38f)) {
+    split_finish(L, a, g, 1);
+    return kFinished;
+  }
+  const float lerr = 0.5f * fast_log2f(fmaxf(err2, 1e-38f));
+  if (err2 <= 1.0f) {
+    const float lf = fminf(kLog2Facc1, fmaxf(kLog2Facc2, fmaf(expo1, lerr, fmaf(-beta, L.lfac_old,
+                                                                                   -kLog2Safe))));
+    R hnew = h * (R)exp2f(-lf);
+    L.lfac_old = fmaxf(lerr, kLog2FacMin);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      L.x[j] = x1[j];
+      if (INTEG == kDopri5) L.kx[j] = kx1[j];
+    }
+    if (joint) {
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        L.v[j] = v1[j];
+        if (INTEG == kDopri5) L.kv[j] = kv1[j];
+      }
+    }
+    if ((double)hnew > c.hmax) hnew = (R)c.hmax;
+    if (L.reject && hnew > h) hnew = h;
+    L.reject = false;
+    if (!clamped || hnew < h) L.h = hnew;
+    L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
+    L.t_gs += (float)h;
+    bool inside = true;
+#pragma unroll
+    for (int j = 0; j < N; j++) inside = inside && (fabs(L.x[j]) <= (R)c.escape);
+    if (!inside) {
+      split_finish(L, a, g, 4);
+      return kFinished;
+    }
+    if (clamped) {
+      if (L.phase == kTransient) {
+        split_start_tangent(L, a, g);
+      } else if (L.phase == kAlign) {
+        if (!split_gram_schmidt(L, a, c, g)) {
+          split_finish(L, a, g, 1);
+          return kFinished;
+        }
+        L.phase = kAverage;
+        L.phase_len = cold_slot().t_avg;
+        L.t_phase = 0.0;
+      } else {
+        const bool ok = split_gram_schmidt(L, a, c, g);
+        split_finish(L, a, g, ok ? 0 : 1);
+        return kFinished;
+      }
+    }
+  } else {
+    L.h = h * (R)exp2f(-fminf(kLog2Facc1, fmaf(expo1, lerr, -kLog2Safe)));
+    L.reject = true;
+  }
+  return kRunning;
+}
+
+}  // namespace adaptive
+}  // namespace chaos

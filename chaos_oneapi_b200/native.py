@@ -19,7 +19,7 @@ INTEG = {"dverk": 0, "dverk65": 1, "dopri5": 2}
 PREC = {"compat": 0, "fp64": 1, "fp32": 2}
 GS = {"cgs": 0, "mgs": 1}
 LAYOUT = {"point": 0, "comp": 1}
-SCHED = {"auto": 0, "direct": 1, "persistent": 2}
+SCHED = {"auto": 0, "direct": 1, "persistent": 2, "split": 3, "split_persistent": 4}
 
 
 class Desc(ctypes.Structure):

@@ -85,7 +85,7 @@ class SweepConfig:
     max_steps: int = 100_000_000
     escape: float = 1e4
     device: int = 0
-    schedule: str = "auto"       # auto | direct | persistent
+    schedule: str = "auto"       # auto | direct | persistent | split | split_persistent
     block: int = 0
     variant: int = 0
     extra: dict = field(default_factory=dict)
@@ -205,7 +205,7 @@ class Sweep:
         b, s = ctypes.c_int32(), ctypes.c_int32()
         check(lib.chaos_lyap_autotune(self._h, sample, _tptr(params, "float64"),
                                       _tptr(inits, "float64"), ctypes.byref(b), ctypes.byref(s)))
-        return {"block": b.value, "schedule": {1: "direct", 2: "persistent"}.get(s.value, "auto"),
+        return {"block": b.value, "schedule": {1: "direct", 2: "persistent", 3: "split", 4: "split_persistent"}.get(s.value, "auto"),
                 "variant": self.variant_in_use()}
 
     def variant_in_use(self) -> int:

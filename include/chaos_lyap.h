@@ -71,8 +71,22 @@ enum { CHAOS_GS_CLASSICAL = 0, CHAOS_GS_MODIFIED = 1 };
  *  COMP_MAJOR:  element (point, c) at a[c * P + point]   (SoA) */
 enum { CHAOS_LAYOUT_POINT_MAJOR = 0, CHAOS_LAYOUT_COMP_MAJOR = 1 };
 
-/* Launch schedule for the adaptive forms. */
-enum { CHAOS_SCHED_AUTO = 0, CHAOS_SCHED_DIRECT = 1, CHAOS_SCHED_PERSISTENT = 2 };
+/* Launch schedule for the adaptive forms of the 3-4-dimensional models.
+ *  DIRECT / PERSISTENT: one lane per point; thread i takes point i, or
+ *    threads pull points from a device work queue.
+ *  SPLIT_DIRECT / SPLIT_PERSISTENT: one point per group of four lanes (each
+ *    lane the state and one tangent vector): about half the work per lane and
+ *    step, for sweeps of few points or runs bounded by their longest point;
+ *    a batch whose first segment's handle has a split schedule runs in the
+ *    split form too.
+ *  AUTO: persistent until chaos_lyap_autotune picks one. */
+enum {
+  CHAOS_SCHED_AUTO = 0,
+  CHAOS_SCHED_DIRECT = 1,
+  CHAOS_SCHED_PERSISTENT = 2,
+  CHAOS_SCHED_SPLIT_DIRECT = 3,
+  CHAOS_SCHED_SPLIT_PERSISTENT = 4
+};
 
 /* Sweep description.  Times are in model time units.  Fields mirror the
  * reference's LyapunovParameters (tool_params.h:23-44): eps = epsilon,
