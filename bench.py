@@ -305,13 +305,15 @@ def run_batch_bench(a, rank, world, local):
     dev = torch.device("cuda", local)
     rng = np.random.default_rng(100 + rank)
     parts, host, sweeps, direct, direct_split = [], [], [], [], []
-    form = "split_persistent" if a.batch_form == "split" else "persistent"
+    def form_of(name):
+        split = a.batch_form == "split" or (a.batch_form == "mixed" and name == "hyper_rossler")
+        return "split_persistent" if split else "persistent"
     for name, seg in BATCH.items():
         params = cl.make_grid(len(seg["base"]), seg["base"], seg["s1"], seg["s2"])
         P = params.shape[0]
         inits = cl.make_inits(len(seg["x0"]), P, seg["x0"], 1e-3, "uniform", rank)
         tavg = rng.uniform(1000.0, 10000.0, P)
-        sw = cl.Sweep(model=name, device=local, schedule=form, **BATCH_KW)
+        sw = cl.Sweep(model=name, device=local, schedule=form_of(name), **BATCH_KW)
         sweeps.append(sw)
         direct.append(cl.Sweep(model=name, device=local, schedule="direct", **BATCH_KW))
         direct_split.append(cl.Sweep(model=name, device=local, schedule="split", **BATCH_KW))
@@ -404,8 +406,9 @@ def run_batch_bench(a, rank, world, local):
                        "points_per_step": total_points, "t_avg": "U[1000, 10000] per point",
                        **{k: v for k, v in BATCH_KW.items() if k != "t_avg"},
                        "launch": "one persistent batch kernel per step, replayed CUDA graph",
-                       "form": ("one point per group of four lanes" if a.batch_form == "split"
-                                else "one point per lane")},
+                       "form": {name: ("one point per group of four lanes"
+                                       if form_of(name).startswith("split") else
+                                       "one point per lane") for name in BATCH}},
             "gpu_launches": a.steps, "clocks": clk,
             "roofline": {"bound": "fp32_fma", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
@@ -444,8 +447,10 @@ def main():
     ap.add_argument("--workload", default="rossler1024",
                     choices=sorted(WORKLOADS) + ["batch256", "surrogate"])
     ap.add_argument("--map-size", type=int, default=4096, help="surrogate workload: cells per side")
-    ap.add_argument("--batch-form", default="split", choices=["split", "lane"],
-                    help="batch256: one point per group of four lanes, or per lane")
+    ap.add_argument("--batch-form", default="mixed", choices=["mixed", "split", "lane"],
+                    help="batch256: every segment one point per lane, every segment one point "
+                         "per group of four lanes, or mixed: the hyperchaotic Rossler segment "
+                         "(whose stiff points set the run's length) split, the others per lane")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-sample", type=int, default=256)
     ap.add_argument("--variant", type=int, default=-1,

@@ -101,36 +101,17 @@ int launch_m(int integ, int prec, const AdaptiveArgs &a, int block, int pblocks,
 
 // ----------------------------------------------------------- mixed batch
 // One persistent launch over segments of different models (3- and
-// 4-dimensional) and per-point averaging times.  A lane holds the state of
-// one point of one model at a time in a union sized for the largest model.
-// Every warp works on one segment at a time (warps start on segments round
-// robin), and a lane that finishes a point takes the next point of its warp's
-// segment: within a segment, lanes refill independently, so uneven point
-// lengths do not strand warps, and since all lanes of a warp run the same
-// model they share one instruction stream.  When its segment has no points
-// left, a lane idles until the whole warp is idle; the warp then moves to the
-// next segment that still has points.  (Letting lanes move on individually
-// mixes models inside warps, which runs every model's step code for the warp
-// and measured slower than three separate launches.)
-template <class R, int INTEG>
-union AnyLane {
-  Lane<Shimizu, 3, R, INTEG> shimizu;
-  Lane<Lorenz, 3, R, INTEG> lorenz;
-  Lane<Rossler, 3, R, INTEG> rossler;
-  Lane<Chua, 3, R, INTEG> chua;
-  Lane<HyperRossler, 4, R, INTEG> hyper;
-};
-
-template <class R, int INTEG, class Fn>
-__device__ __forceinline__ auto visit(int model, AnyLane<R, INTEG> &u, Fn &&fn) {
-  switch (model) {
-    case kShimizu: return fn(u.shimizu);
-    case kLorenz: return fn(u.lorenz);
-    case kRossler: return fn(u.rossler);
-    case kChua: return fn(u.chua);
-    default: return fn(u.hyper);
-  }
-}
+// 4-dimensional) and per-point averaging times.  Every warp works on one
+// segment at a time (warps start on segments round robin); while it does, it
+// runs that segment's model-specific loop -- the sweep kernel's loop with the
+// segment's queue -- so the step code is specialised to the model, with no
+// per-step dispatch, and a lane that finishes a point takes the next point of
+// the segment: lanes refill independently, so uneven point lengths do not
+// strand warps, and all lanes of a warp run one model's instruction stream.
+// When all lanes of the warp are idle (the segment's queue is empty) the warp
+// moves on to the next segment with points left.  (Letting lanes move on
+// individually mixes models inside warps, which runs every model's step code
+// for the warp and measured slower than three separate launches.)
 
 // Next point of segment `seg` for this lane, if any is left.
 __device__ __forceinline__ bool batch_take(const BatchArgs &b, int seg, int64_t &pt) {
@@ -143,62 +124,55 @@ __device__ __forceinline__ bool batch_take(const BatchArgs &b, int seg, int64_t 
   return true;
 }
 
+template <class M, class R, int INTEG>
+__device__ __noinline__ void lane_segment(const BatchArgs &b, int seg, bool active, int64_t pt) {
+  const AdaptiveArgs &a = b.seg[seg];
+  const Ctl c = make_ctl<R>(a);
+  Lane<M, M::N, R, INTEG> L;
+  if (active) lane_start(L, a, pt);
+  while (__any_sync(0xffffffffu, active)) {
+    if (active && lane_step(L, a, c) == kFinished) {
+      active = batch_take(b, seg, pt);
+      if (active) lane_start(L, a, pt);
+    }
+    const bool due = active && L.phase != kTransient && L.t_gs >= L.L;
+    if (__any_sync(0xffffffffu, due)) {
+      if (active && L.phase != kTransient && L.t_gs > 0.f && !lane_gram_schmidt(L, a, c)) {
+        lane_finish(L, a, 1);
+        active = batch_take(b, seg, pt);
+        if (active) lane_start(L, a, pt);
+      }
+    }
+  }
+}
+
 template <class R, int INTEG>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 3 : 1) batch_kernel(const BatchArgs b) {
-  AnyLane<R, INTEG> u;
-  Ctl c{};
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 3 : 1)
+    batch_kernel(const __grid_constant__ BatchArgs b) {
   const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  int wseg = warp % b.nseg;  // the warp's segment (warp-uniform)
-  int tried = 0;             // segments found empty since the warp last got work
-  int64_t pt = 0;
-  auto start = [&]() {
-    c = make_ctl<R>(b.seg[wseg]);
-    visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-      lane_start(L, b.seg[wseg], pt);
-      return 0;
-    });
-  };
-  bool active = batch_take(b, wseg, pt);
-  if (active) start();
-  for (;;) {
-    if (!__any_sync(0xffffffffu, active)) {
-      // the whole warp is idle: next segment with points left, or done
-      if (++tried >= b.nseg) break;
-      wseg = (wseg + 1) % b.nseg;
-      active = batch_take(b, wseg, pt);
-      if (active) start();
+  int wseg = warp % b.nseg;
+  for (int tried = 0; tried < b.nseg; wseg = (wseg + 1) % b.nseg) {
+    int64_t pt = 0;
+    const bool active = batch_take(b, wseg, pt);
+    if (!__any_sync(0xffffffffu, active)) {  // nothing left here for this warp
+      ++tried;
       continue;
     }
     tried = 0;
-    if (active) {
-      const int r = visit<R, INTEG>(b.model[wseg], u,
-                                    [&](auto &L) { return lane_step(L, b.seg[wseg], c); });
-      if (r == kFinished) {
-        active = batch_take(b, wseg, pt);
-        if (active) start();
-      }
-    }
-    const bool due = active && visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-      return L.phase != kTransient && L.t_gs >= L.L;
-    });
-    if (__any_sync(0xffffffffu, due) && active) {
-      const bool failed = visit<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-        if (L.phase == kTransient || !(L.t_gs > 0.f)) return false;
-        if (lane_gram_schmidt(L, b.seg[wseg], c)) return false;
-        lane_finish(L, b.seg[wseg], 1);
-        return true;
-      });
-      if (failed) {
-        active = batch_take(b, wseg, pt);
-        if (active) start();
-      }
+    switch (b.model[wseg]) {
+      case kShimizu: lane_segment<Shimizu, R, INTEG>(b, wseg, active, pt); break;
+      case kLorenz: lane_segment<Lorenz, R, INTEG>(b, wseg, active, pt); break;
+      case kRossler: lane_segment<Rossler, R, INTEG>(b, wseg, active, pt); break;
+      case kChua: lane_segment<Chua, R, INTEG>(b, wseg, active, pt); break;
+      default: lane_segment<HyperRossler, R, INTEG>(b, wseg, active, pt); break;
     }
   }
 }
 
 }  // namespace adaptive
 
-int launch_batch(int integ, int prec, const BatchArgs &b, int block, cudaStream_t s) {
+int launch_batch(int integ, int prec, const BatchArgs &b, int block, cudaStream_t s,
+                 double share, bool high_priority) {
   using namespace adaptive;
   if (b.nseg <= 0 || b.nseg > kMaxSegments) return kErrUnsupported;
   int64_t total = 0;
@@ -220,9 +194,10 @@ int launch_batch(int integ, int prec, const BatchArgs &b, int block, cudaStream_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
-  const int64_t grid = std::min<int64_t>((int64_t)std::max(1, per_sm) * sms, (total + block - 1) / block);
-  kern<<<(unsigned)grid, block, 0, s>>>(b);
-  return (int)cudaGetLastError();
+  const int64_t full = (int64_t)std::max(1, per_sm) * sms;
+  const int64_t cap = std::max<int64_t>(1, (int64_t)(full * std::min(1.0, std::max(share, 0.0))));
+  const int64_t grid = std::min<int64_t>(cap, (total + block - 1) / block);
+  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority, b);
 }
 
 int launch_adaptive(int model, int integ, int prec, const AdaptiveArgs &a, int block,

@@ -113,6 +113,9 @@ struct chaos_lyap_handle {
   int32_t *order = nullptr;
   void *order_scratch = nullptr;
   int64_t order_cap = 0;
+  // second stream and fork / join events of a batch with both kernel forms
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // host-path staging
   double *s_params = nullptr, *s_inits = nullptr, *s_spec = nullptr, *s_tavg = nullptr;
   int32_t *s_status = nullptr;
@@ -279,6 +282,12 @@ int chaos_lyap_destroy(chaos_lyap_handle *h) {
   cudaFree(h->queue);
   cudaFree(h->order);
   cudaFree(h->order_scratch);
+  if (h->aux_stream) {
+    cudaStreamSynchronize(h->aux_stream);
+    cudaStreamDestroy(h->aux_stream);
+  }
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
   cudaStreamDestroy(h->own_stream);
   delete h;
   return CHAOS_LYAP_OK;
@@ -515,12 +524,29 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   return CHAOS_LYAP_OK;
 }
 
-static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArgs *b,
-                       int *integ, int *prec, int *block, bool *split) {
+// A batch runs each segment in the form of its handle's schedule: segments
+// with a split schedule in the split batch kernel, the others in the
+// one-lane batch kernel.  When both kinds are present the two persistent
+// kernels run side by side (forked onto the first handle's second stream,
+// joined before the batch ends; captured as two branches of a graph).  The
+// split kernel -- the form chosen for segments whose longest points set the
+// run's length -- is launched first and at the device's greatest priority
+// with a full machine's grid; the one-lane kernel's blocks take the SM slots
+// that its blocks free as its queues run dry.
+struct BatchPlan {
+  chaos::BatchArgs lane, split;
+  chaos_lyap_handle *lane_h[chaos::kMaxSegments], *split_h[chaos::kMaxSegments];
+  int integ, prec, lane_block, split_block;
+};
+
+static bool is_split(const chaos_lyap_handle *h) {
+  return h->schedule == CHAOS_SCHED_SPLIT_DIRECT || h->schedule == CHAOS_SCHED_SPLIT_PERSISTENT;
+}
+
+static int build_batch(const chaos_lyap_segment *segs, int nseg, BatchPlan *plan) {
   if (!segs || nseg <= 0 || nseg > chaos::kMaxSegments)
     return fail(CHAOS_LYAP_EINVAL, "nseg must be 1..%d", chaos::kMaxSegments);
-  std::memset(b, 0, sizeof *b);
-  b->nseg = nseg;
+  std::memset(plan, 0, sizeof *plan);
   for (int i = 0; i < nseg; i++) {
     const chaos_lyap_segment &sg = segs[i];
     if (!sg.handle) return fail(CHAOS_LYAP_EINVAL, "segment %d: null handle", i);
@@ -534,7 +560,11 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArg
       return fail(CHAOS_LYAP_EINVAL, "segment %d: integrator / precision / device differ", i);
     if (sg.P < 0 || (sg.P > 0 && (!sg.params || !sg.inits || !sg.spectrum)))
       return fail(CHAOS_LYAP_EINVAL, "segment %d: bad arrays", i);
-    chaos::AdaptiveArgs &a = b->seg[i];
+    const bool sp = is_split(sg.handle);
+    chaos::BatchArgs &b = sp ? plan->split : plan->lane;
+    const int j = b.nseg++;
+    (sp ? plan->split_h : plan->lane_h)[j] = sg.handle;
+    chaos::AdaptiveArgs &a = b.seg[j];
     a.P = sg.P;
     a.k = d.k;
     a.gs = d.gs;
@@ -563,44 +593,74 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, chaos::BatchArg
       if (rc) return rc;
       a.order = sg.handle->order;
     }
-    b->model[i] = m->id;
+    b.model[j] = m->id;
   }
-  b->queues = segs[0].handle->queue;
-  const chaos_lyap_desc &d0 = segs[0].handle->d;
-  *integ = d0.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
-  *prec = d0.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
-  *block = segs[0].handle->block;
-  *split = segs[0].handle->schedule == CHAOS_SCHED_SPLIT_DIRECT ||
-           segs[0].handle->schedule == CHAOS_SCHED_SPLIT_PERSISTENT;
+  chaos_lyap_handle *h0 = segs[0].handle;
+  // the first handle's counters: one-lane segments first, then split ones
+  plan->lane.queues = h0->queue;
+  plan->split.queues = h0->queue + plan->lane.nseg;
+  const chaos_lyap_desc &d0 = h0->d;
+  plan->integ = d0.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
+  plan->prec = d0.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
+  plan->lane_block = plan->lane.nseg ? plan->lane_h[0]->block : 128;
+  plan->split_block = plan->split.nseg ? plan->split_h[0]->block : 64;
+  if (plan->lane.nseg && plan->split.nseg && !h0->aux_stream) {  // fork / join resources
+    DeviceGuard g(d0.device);
+    cudaError_t e = cudaStreamCreateWithFlags(&h0->aux_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h0->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h0->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "batch fork stream / events");
+  }
   return CHAOS_LYAP_OK;
 }
 
-static int enqueue_batch(const chaos::BatchArgs &b, const chaos_lyap_segment *segs, int integ,
-                         int prec, int block, bool split, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(b.queues, 0, sizeof(unsigned long long) * b.nseg, s);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
-  int rc;
+static int launch_orders(const chaos::BatchArgs &b, chaos_lyap_handle *const *hs, cudaStream_t s) {
   for (int i = 0; i < b.nseg; i++) {
     if (!b.seg[i].order) continue;
-    rc = chaos::launch_order_longest_first(b.seg[i].t_avg_per_point, b.seg[i].P,
-                                           segs[i].handle->order, segs[i].handle->order_scratch, s);
+    int rc = chaos::launch_order_longest_first(b.seg[i].t_avg_per_point, b.seg[i].P, hs[i]->order,
+                                               hs[i]->order_scratch, s);
     if (rc) return cuda_fail((cudaError_t)rc, "order launch");
   }
-  rc = split ? chaos::launch_batch_split(integ, prec, b, block, s)
-             : chaos::launch_batch(integ, prec, b, block, s);
+  return CHAOS_LYAP_OK;
+}
+
+static int batch_rc(int rc) {
   if (rc == chaos::kErrUnsupported) return fail(CHAOS_LYAP_EUNSUPPORTED, "no batch kernel for this mix");
   if (rc) return cuda_fail((cudaError_t)rc, "batch launch");
   return CHAOS_LYAP_OK;
 }
 
+static int enqueue_batch(const BatchPlan &p, chaos_lyap_handle *h0, cudaStream_t s) {
+  const int nseg = p.lane.nseg + p.split.nseg;
+  cudaError_t e = cudaMemsetAsync(h0->queue, 0, sizeof(unsigned long long) * nseg, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
+  int rc = launch_orders(p.lane, p.lane_h, s);
+  if (!rc) rc = launch_orders(p.split, p.split_h, s);
+  if (rc) return rc;
+  if (p.lane.nseg && p.split.nseg) {
+    cudaStream_t aux = h0->aux_stream;
+    if ((e = cudaEventRecord(h0->ev_fork, s)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(aux, h0->ev_fork, 0)) != cudaSuccess)
+      return cuda_fail(e, "batch fork");
+    rc = batch_rc(chaos::launch_batch_split(p.integ, p.prec, p.split, p.split_block, s, 1.0, true));
+    const int rc2 = batch_rc(chaos::launch_batch(p.integ, p.prec, p.lane, p.lane_block, aux, 1.0));
+    // join even after a failed launch, so that a capture still ends cleanly
+    if ((e = cudaEventRecord(h0->ev_join, aux)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(s, h0->ev_join, 0)) != cudaSuccess)
+      return cuda_fail(e, "batch join");
+    return rc ? rc : rc2;
+  }
+  if (p.split.nseg)
+    return batch_rc(chaos::launch_batch_split(p.integ, p.prec, p.split, p.split_block, s));
+  return batch_rc(chaos::launch_batch(p.integ, p.prec, p.lane, p.lane_block, s));
+}
+
 int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream) {
-  chaos::BatchArgs b;
-  int integ, prec, block;
-  bool split;
-  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block, &split);
+  BatchPlan plan;
+  int rc = build_batch(segs, nseg, &plan);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
-  rc = enqueue_batch(b, segs, integ, prec, block, split, (cudaStream_t)stream);
+  rc = enqueue_batch(plan, segs[0].handle, (cudaStream_t)stream);
   if (!rc) segs[0].handle->last_stream = (cudaStream_t)stream;
   return rc;
 }
@@ -614,10 +674,8 @@ struct chaos_lyap_graph {
 int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chaos_lyap_graph **out) {
   if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
   *out = nullptr;
-  chaos::BatchArgs b;
-  int integ, prec, block;
-  bool split;
-  int rc = build_batch(segs, nseg, &b, &integ, &prec, &block, &split);
+  BatchPlan plan;
+  int rc = build_batch(segs, nseg, &plan);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
   cudaStream_t cs;
@@ -627,13 +685,15 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
   gr->device = segs[0].handle->d.device;
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    rc = enqueue_batch(b, segs, integ, prec, block, split, cs);
+    rc = enqueue_batch(plan, segs[0].handle, cs);
     cudaError_t e2 = cudaStreamEndCapture(cs, &gr->graph);
     if (!rc && e2 != cudaSuccess) rc = cuda_fail(e2, "cudaStreamEndCapture");
   } else {
     rc = cuda_fail(e, "cudaStreamBeginCapture");
   }
-  if (!rc && (e = cudaGraphInstantiate(&gr->exec, gr->graph, 0)) != cudaSuccess)
+  // per-node priorities: the split kernel's blocks are dispatched first
+  if (!rc && (e = cudaGraphInstantiate(&gr->exec, gr->graph, cudaGraphInstantiateFlagUseNodePriority)) !=
+                 cudaSuccess)
     rc = cuda_fail(e, "cudaGraphInstantiate");
   cudaStreamDestroy(cs);
   if (rc) {

@@ -100,13 +100,42 @@ struct BatchArgs {
   unsigned long long *queues;      // nseg point counters, zeroed before the launch
 };
 
-int launch_batch(int integrator, int precision, const BatchArgs &b, int block, cudaStream_t s);
+// share: fraction (0, 1] of a full machine's resident blocks the persistent
+// grid may take; high_priority: launch at the device's greatest stream
+// priority (the block scheduler dispatches its pending blocks first when
+// another batch kernel runs beside it).
+int launch_batch(int integrator, int precision, const BatchArgs &b, int block, cudaStream_t s,
+                 double share = 1.0, bool high_priority = false);
+
+// Kernel launch with an optional priority launch attribute (kept by stream
+// capture as the graph node's priority).
+template <class... Args>
+inline cudaError_t launch_with_priority(void (*kern)(Args...), unsigned grid, unsigned block,
+                                        cudaStream_t s, bool high_priority, Args... args) {
+  if (!high_priority) {
+    kern<<<grid, block, 0, s>>>(args...);
+    return cudaGetLastError();
+  }
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = greatest;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
 
 // Split form (split.cu): one point per group of four lanes.
 int launch_split(int model, int integrator, int precision, const AdaptiveArgs &a, int block,
                  cudaStream_t s);
 int launch_batch_split(int integrator, int precision, const BatchArgs &b, int block,
-                       cudaStream_t s);
+                       cudaStream_t s, double share = 1.0, bool high_priority = false);
 
 }  // namespace chaos
 

@@ -83,30 +83,12 @@ int launch_split_m(int integ, int prec, const AdaptiveArgs &a, int block, cudaSt
 }
 
 // ----------------------------------------------------------- mixed batch
-// The batch kernel of adaptive.cu in the split form: a union of the models'
-// group states; each warp works on one segment at a time (warps start on
-// segments round robin), its groups refill from that segment, and the warp
-// moves on when all its groups are idle.
-template <class R, int INTEG>
-union AnySplit {
-  SplitLane<Shimizu, R, INTEG> shimizu;
-  SplitLane<Lorenz, R, INTEG> lorenz;
-  SplitLane<Rossler, R, INTEG> rossler;
-  SplitLane<Chua, R, INTEG> chua;
-  SplitLane<HyperRossler, R, INTEG> hyper;
-};
-
-template <class R, int INTEG, class Fn>
-__device__ __forceinline__ auto visit_split(int model, AnySplit<R, INTEG> &u, Fn &&fn) {
-  switch (model) {
-    case kShimizu: return fn(u.shimizu);
-    case kLorenz: return fn(u.lorenz);
-    case kRossler: return fn(u.rossler);
-    case kChua: return fn(u.chua);
-    default: return fn(u.hyper);
-  }
-}
-
+// The batch kernel of adaptive.cu in the split form: each warp works on one
+// segment at a time (warps start on segments round robin); while it does, it
+// runs that segment's model-specific loop -- the sweep kernel's loop with the
+// segment's queue -- so the step code is specialised to the model, with no
+// per-step dispatch.  When all groups of the warp are idle (the segment's
+// queue is empty) the warp moves on to the next segment with points left.
 __device__ __forceinline__ bool group_take(const BatchArgs &b, int seg, const Group &g,
                                            int64_t &pt) {
   int64_t v = -1;
@@ -123,55 +105,49 @@ __device__ __forceinline__ bool group_take(const BatchArgs &b, int seg, const Gr
   return v >= 0;
 }
 
+template <class M, class R, int INTEG>
+__device__ __noinline__ void split_segment(const BatchArgs &b, int seg, const Group &g, bool active,
+                              int64_t pt) {
+  const AdaptiveArgs &a = b.seg[seg];
+  const Ctl c = make_ctl<R>(a);
+  SplitLane<M, R, INTEG> L;
+  if (active) split_start(L, a, pt, g);
+  while (__any_sync(0xffffffffu, active)) {
+    if (active && split_step(L, a, c, g) == kFinished) {
+      active = group_take(b, seg, g, pt);
+      if (active) split_start(L, a, pt, g);
+    }
+    const bool due = active && L.phase != kTransient && L.t_gs >= L.L;
+    if (__any_sync(0xffffffffu, due)) {
+      if (active && L.phase != kTransient && L.t_gs > 0.f && !split_gram_schmidt(L, a, c, g)) {
+        split_finish(L, a, g, 1);
+        active = group_take(b, seg, g, pt);
+        if (active) split_start(L, a, pt, g);
+      }
+    }
+  }
+}
+
 template <class R, int INTEG>
-__global__ void __launch_bounds__(128) batch_split_kernel(const BatchArgs b) {
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 2)
+    batch_split_kernel(const __grid_constant__ BatchArgs b) {
   const Group g = group_of();
-  AnySplit<R, INTEG> u;
-  Ctl c{};
   const int warp = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   int wseg = warp % b.nseg;
-  int tried = 0;
-  int64_t pt = 0;
-  auto start = [&]() {
-    c = make_ctl<R>(b.seg[wseg]);
-    visit_split<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-      split_start(L, b.seg[wseg], pt, g);
-      return 0;
-    });
-  };
-  bool active = group_take(b, wseg, g, pt);
-  if (active) start();
-  for (;;) {
-    if (!__any_sync(0xffffffffu, active)) {
-      if (++tried >= b.nseg) break;
-      wseg = (wseg + 1) % b.nseg;
-      active = group_take(b, wseg, g, pt);
-      if (active) start();
+  for (int tried = 0; tried < b.nseg; wseg = (wseg + 1) % b.nseg) {
+    int64_t pt = 0;
+    const bool active = group_take(b, wseg, g, pt);
+    if (!__any_sync(0xffffffffu, active)) {  // nothing left here for this warp
+      ++tried;
       continue;
     }
     tried = 0;
-    if (active) {
-      const int r = visit_split<R, INTEG>(b.model[wseg], u,
-                                          [&](auto &L) { return split_step(L, b.seg[wseg], c, g); });
-      if (r == kFinished) {
-        active = group_take(b, wseg, g, pt);
-        if (active) start();
-      }
-    }
-    const bool due = active && visit_split<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-      return L.phase != kTransient && L.t_gs >= L.L;
-    });
-    if (__any_sync(0xffffffffu, due) && active) {
-      const bool failed = visit_split<R, INTEG>(b.model[wseg], u, [&](auto &L) {
-        if (L.phase == kTransient || !(L.t_gs > 0.f)) return false;
-        if (split_gram_schmidt(L, b.seg[wseg], c, g)) return false;
-        split_finish(L, b.seg[wseg], g, 1);
-        return true;
-      });
-      if (failed) {
-        active = group_take(b, wseg, g, pt);
-        if (active) start();
-      }
+    switch (b.model[wseg]) {
+      case kShimizu: split_segment<Shimizu, R, INTEG>(b, wseg, g, active, pt); break;
+      case kLorenz: split_segment<Lorenz, R, INTEG>(b, wseg, g, active, pt); break;
+      case kRossler: split_segment<Rossler, R, INTEG>(b, wseg, g, active, pt); break;
+      case kChua: split_segment<Chua, R, INTEG>(b, wseg, g, active, pt); break;
+      default: split_segment<HyperRossler, R, INTEG>(b, wseg, g, active, pt); break;
     }
   }
 }
@@ -193,7 +169,8 @@ int launch_split(int model, int integ, int prec, const AdaptiveArgs &a, int bloc
   }
 }
 
-int launch_batch_split(int integ, int prec, const BatchArgs &b, int block, cudaStream_t s) {
+int launch_batch_split(int integ, int prec, const BatchArgs &b, int block, cudaStream_t s,
+                       double share, bool high_priority) {
   using namespace adaptive;
   if (b.nseg <= 0 || b.nseg > kMaxSegments) return kErrUnsupported;
   int64_t total = 0;
@@ -216,9 +193,10 @@ int launch_batch_split(int integ, int prec, const BatchArgs &b, int block, cudaS
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
   const int64_t groups = block / kSplitLanes;
-  const int64_t grid = std::min<int64_t>((int64_t)std::max(1, per_sm) * sms, (total + groups - 1) / groups);
-  kern<<<(unsigned)grid, block, 0, s>>>(b);
-  return (int)cudaGetLastError();
+  const int64_t full = (int64_t)std::max(1, per_sm) * sms;
+  const int64_t cap = std::max<int64_t>(1, (int64_t)(full * std::min(1.0, std::max(share, 0.0))));
+  const int64_t grid = std::min<int64_t>(cap, (total + groups - 1) / groups);
+  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority, b);
 }
 
 }  // namespace chaos

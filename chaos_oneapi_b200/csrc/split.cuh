@@ -83,7 +83,7 @@ template <class M, class R, int INTEG>
 __device__ void split_finish(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Group &g,
                              int status) {
   const Cold &c = cold_slot();
-  if (g.r < a.k) {
+  if (g.r < M::N) {
     split_flush(L);
     const double lam = status ? quiet_nan() : c.sum[0] / c.t_avg;
     a.spectrum.base[c.pt * a.spectrum.ps + g.r * a.spectrum.cs] = lam;
@@ -99,7 +99,7 @@ __device__ void split_start_tangent(SplitLane<M, R, INTEG> &L, const AdaptiveArg
                                     const Group &g) {
   constexpr int N = M::N;
 #pragma unroll
-  for (int j = 0; j < N; j++) L.v[j] = (j == g.r && g.r < a.k) ? R(1) : R(0);
+  for (int j = 0; j < N; j++) L.v[j] = (j == g.r) ? R(1) : R(0);
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
   L.lfac_old = kLog2FacMin;
   L.t_phase = 0.0;
@@ -201,7 +201,7 @@ template <class M, class R, int INTEG>
 __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a,
                                    const Ctl &c, const Group &g) {
   constexpr int N = M::N;
-  const int k = a.k;
+  constexpr int k = M::N;  // launches take k == dim
   const bool has_vec = g.r < k;
   double vo[N], w[N];
   R before = 0;
@@ -214,8 +214,7 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
   double rr = 1.0;
   float cancel = 1.0f;
 #pragma unroll
-  for (int q = 0; q < N; q++) {
-    if (q >= k) break;  // k is the same in all lanes
+  for (int q = 0; q < k; q++) {
     if (g.r == q) {
       double s = 0;
 #pragma unroll
@@ -284,7 +283,7 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
   const bool clamped = (double)L.h >= remaining;
   const R h = clamped ? (R)remaining : L.h;
   const bool joint = L.phase != kTransient;
-  const bool has_vec = g.r < a.k;
+  const bool has_vec = g.r < M::N;  // launches take k == dim
   R x1[N], v1[N], kx1[N], kv1[N];
   L.steps++;
   const float err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, c.rtol, c.atol, x1, v1,

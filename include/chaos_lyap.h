@@ -76,9 +76,10 @@ enum { CHAOS_LAYOUT_POINT_MAJOR = 0, CHAOS_LAYOUT_COMP_MAJOR = 1 };
  *    threads pull points from a device work queue.
  *  SPLIT_DIRECT / SPLIT_PERSISTENT: one point per group of four lanes (each
  *    lane the state and one tangent vector): about half the work per lane and
- *    step, for sweeps of few points or runs bounded by their longest point;
- *    a batch whose first segment's handle has a split schedule runs in the
- *    split form too.
+ *    step, for sweeps of few points or runs bounded by their longest point.
+ *    A batch runs each segment in the form of its handle's schedule; with
+ *    both forms present the two batch kernels run side by side, the split
+ *    one first and at the greatest stream priority.
  *  AUTO: persistent until chaos_lyap_autotune picks one. */
 enum {
   CHAOS_SCHED_AUTO = 0,

@@ -132,7 +132,7 @@ def test_split_per_point_times_longest_first(lib, orc):
     np.testing.assert_allclose(got[settle], ref[settle], rtol=0, atol=1e-3)
 
 
-def test_batch_split_matches_one_lane_batch(lib, orc):
+def test_batch_split_and_mixed_match_one_lane_batch(lib, orc):
     import torch
     segs = {
         "lorenz": ([10.0, 28.0, 8.0 / 3.0], [0, 5, 20, 8], [1, 0, 200, 8], [1.0, 1.0, 1.0]),
@@ -151,10 +151,13 @@ def test_batch_split_matches_one_lane_batch(lib, orc):
         P = params.shape[0]
         inputs.append((name, params, orc.make_inits(len(x0), P, x0, 1e-3, 0, 1),
                        rng.uniform(10.0, 40.0, P)))
-    for schedule in ("persistent", "split_persistent"):
+    forms = {"lane": lambda n: "persistent", "split": lambda n: "split_persistent",
+             # both batch kernels side by side on forked streams
+             "mixed": lambda n: "split_persistent" if n == "hyper_rossler" else "persistent"}
+    for form, schedule_of in forms.items():
         parts, sweeps = [], []
         for name, params, inits, tavg in inputs:
-            sw = lib.Sweep(model=name, schedule=schedule, **kw)
+            sw = lib.Sweep(model=name, schedule=schedule_of(name), **kw)
             sweeps.append(sw)
             P = params.shape[0]
             dev = [torch.from_numpy(a).cuda() for a in (params, inits, tavg)]
@@ -164,12 +167,16 @@ def test_batch_split_matches_one_lane_batch(lib, orc):
         g = lib.BatchGraph(parts)
         g.launch()
         torch.cuda.synchronize()
-        out[schedule] = [(pt[3].cpu().numpy(), pt[4].cpu().numpy()) for pt in parts]
+        out[form] = [(pt[3].cpu().numpy(), pt[4].cpu().numpy()) for pt in parts]
         g.close()
         for sw in sweeps:
             sw.close()
-    for (name, params, _, _), (s1, st1), (s2, st2) in zip(inputs, out["persistent"],
-                                                           out["split_persistent"]):
+    for other in ("split", "mixed"):
+        _compare_batches(inputs, out["lane"], out[other])
+
+
+def _compare_batches(inputs, ref, got):
+    for (name, params, _, _), (s1, st1), (s2, st2) in zip(inputs, ref, got):
         assert (st1 >= 0).all() and (st2 >= 0).all()
         assert (st1 == st2).mean() > 0.95
         ok = (st1 == 0) & (st2 == 0)
