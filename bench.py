@@ -1,7 +1,7 @@
 """Throughput of the Lyapunov-spectrum sweep.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rossler1024|lorenz64|l96_256|batch256]
+                    [--workload rossler1024|lorenz64|lorenz1024|l96_256|batch256|surrogate]
 
 Workload (default ``rossler1024``, the precision form): Rossler
 dx = -y - z, dy = x + a y, dz = b + z (x - c), b = 0.2, on a 1024 x 1024 grid
@@ -11,7 +11,11 @@ point; Dormand-Prince 5(4) with state and tangent in FP32 (rtol = atol =
 500, averaging 5000 time units, renormalisation every 2.  One step = the
 whole map.  ``lorenz64``: Lorenz 64 x 64, sigma in [5, 20] x rho in [0, 200],
 beta = 8/3, DVERK 6(5) FP64 rtol = atol = 1e-10, transient 100, averaging
-1000, renormalisation every 1.
+1000, renormalisation every 1.  ``lorenz1024``: the same Lorenz ranges on a
+1024 x 1024 grid in the precision form (FP32 Dopri5 rtol 1e-6, FP64
+renormalisation), with the plain FP64 DVERK 6(5) rtol 1e-10 sweep of the same
+map timed once in the same run; the line reports the time ratio and both
+forms' errors against the FP64 rtol 1e-12 oracle.
 
 Under torchrun each rank sweeps its own map (jitter seed = rank): weak
 scaling, no collective on the data path; the reported time is the maximum
@@ -55,6 +59,14 @@ WORKLOADS = {
         x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dverk65", precision="fp64", rtol=1e-10,
         atol=1e-10, h=1e-3, t_transient=100.0, t_avg=1000.0, dt_renorm=1.0, dtype="fp64",
         ref_h=1e-3, ref_cost=0.32),
+    # precision form on the Lorenz map: FP32 Dopri5 against the plain FP64
+    # DVERK 6(5) sweep of the same 1024^2 map, timed in the same run
+    "lorenz1024": dict(
+        model="lorenz", base=[10.0, 28.0, 8.0 / 3.0], s1=[0, 5.0, 20.0, 1024],
+        s2=[1, 0.0, 200.0, 1024], x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dopri5",
+        precision="fp32", rtol=1e-6, atol=1e-6, h=1e-3, t_transient=100.0, t_avg=1000.0,
+        dt_renorm=1.0, dtype="fp32", ref_h=1e-3, ref_cost=0.32,
+        plain=dict(integrator="dverk65", precision="fp64", rtol=1e-10, atol=1e-10)),
     # warp-per-point form: Lorenz-96, N = 40, full 40-exponent spectrum
     "l96_256": dict(
         model="lorenz96", base=[8.0, 1.0], s1=[0, 4.0, 16.0, 256], s2=[1, 0.5, 1.5, 256],
@@ -260,7 +272,17 @@ def run_surrogate_bench(a, rank, world, local):
     plain_sweep(sw, spec, sample)
     plain_est = (time.perf_counter() - t0) * P / sample.size
     cfg = RefineConfig(steps0=6000, steps_round=4000, rounds=4, round_grid_step=max(1, n // 512),
-                       round_max_new=65536)
+                       round_max_new=65536, rule=a.surrogate_rule)
+    if cfg.rule == "regime":
+        cfg.lam_limit = 0.005
+        rule = (f"integrate where the ensemble's regime score r = tanh((lambda_1 - "
+                f"{cfg.regime_threshold}) / {cfg.regime_width}) is not confident "
+                f"(|mean r| < {cfg.regime_conf} or std r > {cfg.regime_std}), disagrees with "
+                f"the sign of mean lambda_1 - {cfg.regime_threshold}, or mean lambda_1 is within "
+                f"{cfg.lam_limit} of {cfg.regime_threshold}")
+    else:
+        rule = (f"integrate where std(lambda_1) > {cfg.std_limit} or |lambda_1| < "
+                f"{cfg.lam_limit}")
     clocks = ClockSampler(local)
     clocks.start()
     out, mask, info = refine_map(spec, sw, cfg)
@@ -280,7 +302,7 @@ def run_surrogate_bench(a, rank, world, local):
                        "plain": "DVERK 6(5) FP64 rtol 1e-10, T 100 + 1000, renorm 1",
                        "ensemble": "4 x MLP 16 Fourier features -> 128 -> 128 -> 128 -> 3, "
                                    "SiLU, BF16 mma.sync, FP32 accumulate, Adam 1e-3",
-                       "rule": "integrate where std(lambda_1) > 0.02 or |lambda_1| < 0.05",
+                       "rule": rule,
                        "rounds": cfg.rounds, "round_max_new": cfg.round_max_new},
             "refined_s": refined, "plain_estimate_s": plain_est,
             "refined_over_plain": refined / plain_est,
@@ -425,6 +447,28 @@ def run_batch_bench(a, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def accuracy_vs(spec, status, ref, rst):
+    """Per-exponent error of `spec` against the oracle's `ref` on the points
+    both integrated to the end (status 0)."""
+    ok = (rst == 0) & (status == 0)
+    d = np.abs(spec[ok] - ref[ok])
+    chaotic = ref[ok][:, 0] > 0.01
+    return {
+        "sample": int(len(status)), "compared": int(ok.sum()),
+        "status_agree": float((rst == status).mean()),
+        "frac_all_within_1e-3": float((d.max(axis=1) <= 1e-3).mean()),
+        "frac_within_1e-3_per_exponent": [float(x) for x in (d <= 1e-3).mean(axis=0)][:8],
+        "median_abs_err": [float(x) for x in np.median(d, axis=0)][:8],
+        "max_abs_err_regular": ([float(x) for x in d[~chaotic].max(axis=0)][:8]
+                                if (~chaotic).any() else None),
+        "frac_regular_within_1e-3": (float((d[~chaotic].max(axis=1) <= 1e-3).mean())
+                                     if (~chaotic).any() else None),
+        "chaotic_cells": int(chaotic.sum()),
+        "regime_sign_agreement": float((np.sign(spec[ok][:, 0] - 0.01) ==
+                                        np.sign(ref[ok][:, 0] - 0.01)).mean()),
+    }
+
+
 def config_of(a, w, extra=None):
     c = {"workload": a.workload, "model": w["model"], "exponents": w.get("k", 3),
          "grid": f"{int(w['s1'][3])}x{int(w['s2'][3])}",
@@ -451,6 +495,8 @@ def main():
                     help="batch256: every segment one point per lane, every segment one point "
                          "per group of four lanes, or mixed: the hyperchaotic Rossler segment "
                          "(whose stiff points set the run's length) split, the others per lane")
+    ap.add_argument("--surrogate-rule", default="regime", choices=["regime", "spread"],
+                    help="surrogate: which cells the plain sweep integrates (see RefineConfig)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-sample", type=int, default=256)
     ap.add_argument("--variant", type=int, default=-1,
@@ -591,6 +637,35 @@ def main():
            "h2d_bytes_per_step": int(hp.numel() * 8 + hx.numel() * 8),
            "d2h_bytes_per_step": int(hs.numel() * 8 + hst.numel() * 4), "steps": e2e_steps}
 
+    # the plain FP64 sweep of the same map (one timed run after the autotuner's
+    # warm launches), for the precision form's time ratio
+    plain = None
+    if "plain" in w:
+        psw = cl.Sweep(**dict(common, **w["plain"]))
+        ptuned = psw.autotune(dp, dx, sample=min(P, 1 << 17))
+        pds = torch.empty_like(ds)
+        pst = torch.empty_like(st)
+        psteps = torch.empty_like(steps)
+        with torch.cuda.stream(stream):
+            flush.fill_(0x5A)
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize(dev)
+            p0.record(stream)
+            psw.run(dp, dx, pds, pst, psteps, stream=stream)
+            p1.record(stream)
+            stream.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+        if world > 1:
+            t = torch.tensor([plain_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            plain_ms = t.item()
+        psw.close()
+        plain = {"ms": plain_ms, "launch": ptuned, "spec": pds.cpu().numpy(),
+                 "status": pst.cpu().numpy(), "steps": psteps.cpu().numpy()}
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -623,6 +698,24 @@ def main():
                    "steps_mean": float(steps_np.mean()), "steps_max": int(steps_np.max())},
     }
 
+    if plain is not None:
+        form_ms = elapsed_ms / a.steps
+        both = (status_np == 0) & (plain["status"] == 0)
+        dd = np.abs(spec_np[both] - plain["spec"][both])
+        line["vs_plain_fp64"] = {
+            "plain": {"integrator": w["plain"]["integrator"], "precision": "fp64",
+                      "rtol": w["plain"]["rtol"], "launch": plain["launch"]},
+            "plain_s": plain["ms"] * 1e-3, "form_s": form_ms * 1e-3,
+            "time_ratio_plain_over_form": plain["ms"] / form_ms,
+            "plain_points_per_s": P * world / (plain["ms"] * 1e-3),
+            "plain_steps_mean": float(plain["steps"].mean()),
+            "whole_map_vs_plain": {
+                "compared": int(both.sum()),
+                "status_agree": float((status_np == plain["status"]).mean()),
+                "frac_all_within_1e-3": float((dd.max(axis=1) <= 1e-3).mean()),
+                "regime_sign_agreement": float((np.sign(spec_np[both][:, 0] - 0.01) ==
+                                                np.sign(plain["spec"][both][:, 0] - 0.01)).mean())},
+        }
     # accuracy against the FP64 oracle (rtol 1e-12) on a random sample
     if w["model"] == "lorenz96":  # exact on every point: sum(lambda) = -N gamma
         okp = status_np == 0
@@ -640,22 +733,11 @@ def main():
                                       gs=w.get("gs", "cgs"), rtol=orc_rtol, atol=orc_rtol,
                                       t_transient=w["t_transient"], t_avg=w["t_avg"],
                                       dt_renorm=w["dt_renorm"])
-        ok = (rst == 0) & (status_np[idx] == 0)
-        d = np.abs(spec_np[idx][ok] - ref[ok])
-        chaotic = ref[ok][:, 0] > 0.01
-        line["accuracy"] = {
-            "vs": f"FP64 adaptive oracle, rtol=atol={orc_rtol:g} (CPU)",
-            "sample": int(sample), "compared": int(ok.sum()),
-            "status_agree": float((rst == status_np[idx]).mean()),
-            "frac_all_within_1e-3": float((d.max(axis=1) <= 1e-3).mean()),
-            "frac_within_1e-3_per_exponent": [float(x) for x in (d <= 1e-3).mean(axis=0)][:8],
-            "median_abs_err": [float(x) for x in np.median(d, axis=0)][:8],
-            "max_abs_err_regular": ([float(x) for x in d[~chaotic].max(axis=0)][:8]
-                                    if (~chaotic).any() else None),
-            "chaotic_cells": int(chaotic.sum()),
-            "regime_sign_agreement": float((np.sign(spec_np[idx][ok][:, 0] - 0.01) ==
-                                            np.sign(ref[ok][:, 0] - 0.01)).mean()),
-        }
+        line["accuracy"] = dict(vs=f"FP64 adaptive oracle, rtol=atol={orc_rtol:g} (CPU)",
+                                **accuracy_vs(spec_np[idx], status_np[idx], ref, rst))
+        if plain is not None:
+            line["vs_plain_fp64"]["accuracy"] = accuracy_vs(plain["spec"][idx],
+                                                            plain["status"][idx], ref, rst)
 
     if not a.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -8,10 +8,10 @@ cells where it is confident, and the plain sweep integrates the rest:
 1. plain sweep of a coarse training grid (e.g. 128 x 128);
 2. train the ensemble;
 3. refinement rounds: predict on a candidate subgrid of the fine map, pick
-   cells where the ensemble's spread of lambda_1 exceeds std_limit or the
-   predicted |lambda_1| is below lam_limit (regime boundaries, periodic
-   windows), integrate (a capped number of) them plainly, add them to the
-   training data, fine-tune;
+   the cells the rule flags (RefineConfig.rule: the ensemble's spread of
+   lambda_1 and a near-zero band, or the ensemble's confidence in its call
+   of the regime near lambda_1 = 0+), integrate (a capped number of) them
+   plainly, add them to the training data, fine-tune;
 4. final fill: predict the whole fine map; integrate plainly every cell the
    same rule flags; the surrogate's mean fills the rest.
 
@@ -200,8 +200,21 @@ class RefineConfig:
     rounds: int = 2
     round_grid_step: int = 8       # candidates: every k-th cell of the fine map
     round_max_new: int = 32768     # cells integrated per refinement round
+    # Which cells the plain sweep integrates.  "spread": the ensemble's std
+    # of lambda_1 above std_limit or the predicted |lambda_1| below
+    # lam_limit.  "regime": the networks also learn a regime score
+    # r = tanh((lambda_1 - regime_threshold) / regime_width) (a fourth
+    # output); a cell is integrated where the ensemble's call of the regime
+    # is not confident (|mean r| < regime_conf or std r > regime_std) or
+    # disagrees with the sign of its own mean lambda_1 - regime_threshold, or
+    # where the predicted lambda_1 lies within lam_limit of the threshold.
+    rule: str = "spread"
     std_limit: float = 0.02        # ensemble std of lambda_1
-    lam_limit: float = 0.05        # predicted |lambda_1|
+    lam_limit: float = 0.05        # predicted |lambda_1| ("spread"); |lambda_1 - thr| ("regime")
+    regime_threshold: float = 0.01
+    regime_width: float = 0.005
+    regime_conf: float = 0.5
+    regime_std: float = 0.2
     seed: int = 0
     timings: dict = field(default_factory=dict)
 
@@ -225,7 +238,22 @@ def plain_sweep(sweep: Sweep, spec: MapSpec, index: np.ndarray, chunk: int = 1 <
 
 
 def _flags(mean, std, cfg):
-    return (std[:, 0] > cfg.std_limit) | (mean[:, 0].abs() < cfg.lam_limit)
+    if cfg.rule == "spread":
+        return (std[:, 0] > cfg.std_limit) | (mean[:, 0].abs() < cfg.lam_limit)
+    if cfg.rule != "regime":
+        raise ValueError(f"unknown rule {cfg.rule!r}")
+    r, rs = mean[:, -1], std[:, -1]
+    lam = mean[:, 0] - cfg.regime_threshold
+    return ((r.abs() < cfg.regime_conf) | (rs > cfg.regime_std) | ((r > 0) != (lam > 0))
+            | (lam.abs() < cfg.lam_limit))
+
+
+def _targets(y, cfg):
+    """Training targets: the spectrum, plus the regime score for "regime"."""
+    if cfg.rule != "regime":
+        return y
+    r = np.tanh((y[:, 0] - cfg.regime_threshold) / cfg.regime_width)
+    return np.concatenate([y, r[:, None]], axis=1)
 
 
 def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None):
@@ -254,15 +282,17 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None):
 
     # 2. train
     t = time.perf_counter()
-    net = MLPEnsemble(cfg.ensemble, cfg.width, k, cfg.seed, sweep.cfg.device)
+    outs = k + (1 if cfg.rule == "regime" else 0)
+    net = MLPEnsemble(cfg.ensemble, cfg.width, outs, cfg.seed, sweep.cfg.device)
     net.set_domain(spec.sweep1[1], spec.sweep1[2], spec.sweep2[1], spec.sweep2[2])
     if cfg.feature_scale > 0:
         net.set_features(np.random.default_rng(cfg.seed + 99).normal(0, cfg.feature_scale, (8, 2)))
-    net.set_target_scale(y.mean(0), y.std(0) + 1e-6)
+    yt = _targets(y, cfg)
+    net.set_target_scale(yt.mean(0), yt.std(0) + 1e-6)
 
     def fit(idx, targets, steps, seed):
         xy = torch.from_numpy(spec.coords(idx)).cuda()
-        T = torch.from_numpy(np.ascontiguousarray(targets)).cuda()
+        T = torch.from_numpy(np.ascontiguousarray(_targets(targets, cfg))).cuda()
         loss = None
         for j, f in enumerate(cfg.lr_phases):
             n = steps // len(cfg.lr_phases)
@@ -309,7 +339,7 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None):
         xy = torch.from_numpy(spec.coords(idx)).cuda()
         mean, std = net.predict(xy)
         f = _flags(mean, std, cfg)
-        out[o:o + idx.size] = mean.double().cpu().numpy()
+        out[o:o + idx.size] = mean[:, :k].double().cpu().numpy()
         flagged.append(idx[f.cpu().numpy()])
     torch.cuda.synchronize()
     tm["predict_s"] = time.perf_counter() - t

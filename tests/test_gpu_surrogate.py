@@ -60,17 +60,20 @@ def test_training_fits_a_smooth_map(lib):
     net.close()
 
 
-def test_refined_map_against_plain_on_held_out_cells(lib):
+@pytest.mark.parametrize("rule", ["spread", "regime"])
+def test_refined_map_against_plain_on_held_out_cells(lib, rule):
     """A 256 x 256 Lorenz map (short horizon): the refined map integrates a
     fraction of the cells and agrees with the plain sweep on the regime of
-    held-out cells."""
+    held-out cells, under either cell-selection rule."""
     from chaos_oneapi_b200.surrogate import MapSpec, RefineConfig, plain_sweep, refine_map
     spec = MapSpec("lorenz", [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, 256], [1, 0.0, 200.0, 256],
                    [1.0, 1.0, 1.0], seed=4)
     sw = lib.Sweep(model="lorenz", method="var", integrator="dverk65", precision="fp64",
                    rtol=1e-8, atol=1e-8, h=1e-3, t_transient=20.0, t_avg=300.0, dt_renorm=1.0)
     cfg = RefineConfig(train_grid=64, steps0=3000, steps_round=1500, rounds=2, round_grid_step=2,
-                       round_max_new=8192)
+                       round_max_new=8192, rule=rule)
+    if rule == "regime":
+        cfg.lam_limit = 0.005
     out, mask, info = refine_map(spec, sw, cfg)
     rng = np.random.default_rng(11)
     held = rng.choice(256 * 256, 1000, replace=False)
