@@ -285,13 +285,30 @@ def run_surrogate_bench(a, rank, world, local):
                 f"{cfg.lam_limit}")
     clocks = ClockSampler(local)
     clocks.start()
-    out, mask, info = refine_map(spec, sw, cfg)
+    out, mask, info = refine_map(spec, sw, cfg, probe=held)
     clk = clocks.stop()
+    pm, ps = info.pop("probe_mean"), info.pop("probe_std")
     refined = info["timings"]["total_s"]
     ok = st == 0
     agree = float(((out[held, 0] > 0.01) == (truth[:, 0] > 0.01))[ok].mean())
     d = np.abs(out[held] - truth)[ok]
     filled = ~mask[held][ok]
+    # the same trained ensemble under other thresholds of the rule: the
+    # fraction of held-out cells each would send to the plain sweep and the
+    # regime agreement it would reach (a flagged cell takes the plain value)
+    sens = []
+    if cfg.rule == "regime":
+        import torch
+        from chaos_oneapi_b200.surrogate import _flags
+        for conf, sd in ((0.5, 0.2), (0.7, 0.15), (0.8, 0.1), (0.9, 0.05)):
+            c2 = RefineConfig(**{**cfg.__dict__, "regime_conf": conf, "regime_std": sd,
+                                 "timings": {}})
+            fl = _flags(torch.from_numpy(pm), torch.from_numpy(ps), c2).numpy() | mask[held]
+            pred = np.where(fl, truth[:, 0], pm[:, 0])
+            sens.append({"regime_conf": conf, "regime_std": sd,
+                         "plain_fraction": float(fl.mean()),
+                         "regime_agreement": float(((pred > 0.01) == (truth[:, 0] > 0.01))[ok]
+                                                   .mean())})
     if rank == 0:
         line = {
             "metric": METRIC + " (surrogate-refined map)", "value": P / refined, "unit": "points/s",
@@ -311,7 +328,10 @@ def run_surrogate_bench(a, rank, world, local):
             "held_out": {"cells": int(ok.sum()), "regime_agreement": agree,
                          "surrogate_filled": int(filled.sum()),
                          "median_abs_err_filled": ([float(x) for x in np.median(d[filled], 0)]
-                                                   if filled.any() else None)},
+                                                   if filled.any() else None),
+                         "p99_abs_err_filled": ([float(x) for x in np.quantile(d[filled], 0.99, 0)]
+                                                if filled.any() else None)},
+            "rule_thresholds_on_held_out": sens,
             "gpu_launches": None,
         }
         print(json.dumps(line), flush=True)

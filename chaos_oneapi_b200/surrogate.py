@@ -213,8 +213,8 @@ class RefineConfig:
     lam_limit: float = 0.05        # predicted |lambda_1| ("spread"); |lambda_1 - thr| ("regime")
     regime_threshold: float = 0.01
     regime_width: float = 0.005
-    regime_conf: float = 0.5
-    regime_std: float = 0.2
+    regime_conf: float = 0.7
+    regime_std: float = 0.15
     seed: int = 0
     timings: dict = field(default_factory=dict)
 
@@ -256,9 +256,12 @@ def _targets(y, cfg):
     return np.concatenate([y, r[:, None]], axis=1)
 
 
-def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None):
+def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None, probe=None):
     """Runs the whole pipeline.  Returns (spectrum map P x k float64, plain
-    mask P bool, info dict with stage timings and counts)."""
+    mask P bool, info dict with stage timings and counts).  With `probe`
+    (flat cell indices), info also holds the final ensemble's mean and std
+    on those cells ("probe_mean", "probe_std", numpy), after the timed
+    pipeline."""
     import torch
     t_all = time.perf_counter()
     tm = {}
@@ -356,5 +359,8 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None):
     info = {"timings": tm, "points": P, "plain_cells": int(mask.sum()),
             "plain_fraction": float(mask.mean()), "training_cells": int(train_idx.size),
             "final_flagged": int(flagged.size)}
+    if probe is not None:
+        mean, std = net.predict(torch.from_numpy(spec.coords(np.asarray(probe))).cuda())
+        info["probe_mean"], info["probe_std"] = mean.cpu().numpy(), std.cpu().numpy()
     net.close()
     return out, mask, info

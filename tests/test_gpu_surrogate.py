@@ -73,7 +73,7 @@ def test_refined_map_against_plain_on_held_out_cells(lib, rule):
     cfg = RefineConfig(train_grid=64, steps0=3000, steps_round=1500, rounds=2, round_grid_step=2,
                        round_max_new=8192, rule=rule)
     if rule == "regime":
-        cfg.lam_limit = 0.005
+        cfg.lam_limit = 0.005  # around the regime threshold 0.01
     out, mask, info = refine_map(spec, sw, cfg)
     rng = np.random.default_rng(11)
     held = rng.choice(256 * 256, 1000, replace=False)
