@@ -46,6 +46,7 @@ const ModelInfo kModels[] = {
     {"chua", chaos::kChua, 3, 4, 0, "alpha, beta, m0, m1", "x, y, z",
      "x' = alpha * (y - x - f(x));y' = x - y + z;z' = - beta * y;"
      "f(x) = m1 * x + 0.5 * (m0 - m1) * (|x + 1| - |x - 1|)"},
+    {"henon", chaos::kHenon, 2, 2, 1, "a, b", "x, y", "x -> 1 - a * x^2 + y;y -> b * x"},
     {"hyper_rossler", chaos::kHyperRossler, 4, 2, 0, "c, d", "x, y, z, w",
      "x' = - y - z;y' = x + 0.25 * y + w;z' = 3 + x * z;w' = - c * z + d * w"},
     {"lorenz", chaos::kLorenz, 3, 3, 0, "sigma, rho, beta", "x, y, z",
@@ -217,7 +218,14 @@ static int check_desc(const chaos_lyap_desc *d, const ModelInfo **mout) {
   } else {
     return fail(CHAOS_LYAP_EINVAL, "bad precision %d", d->precision);
   }
-  if (m->type != 0) return fail(CHAOS_LYAP_EUNSUPPORTED, "map models are not provided");
+  if (m->type != 0) {  // maps: the reference's FD / VAR map branches, in compat precision
+    if (d->precision != CHAOS_PREC_COMPAT_FP64)
+      return fail(CHAOS_LYAP_EUNSUPPORTED,
+                  "map model %s: maps are iterated, not integrated; use compat precision", m->name);
+    if (d->method == CHAOS_METHOD_QR)
+      return fail(CHAOS_LYAP_EUNSUPPORTED, "map model %s: the QR method has no map branch",
+                  m->name);
+  }
   return CHAOS_LYAP_OK;
 }
 
@@ -738,8 +746,11 @@ int chaos_lyap_cudaLyapunov(int bn, int bs, size_t taskNum, int isQr, int isVar,
   (void)bs;
   const ModelInfo *m = find_model(model);
   if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", model ? model : "(null)");
-  if (modelType != 0 || m->type != 0)
-    return fail(CHAOS_LYAP_EUNSUPPORTED, "map models are not provided");
+  if (modelType != m->type)
+    return fail(CHAOS_LYAP_EINVAL, "model %s is a %s, modelType %d", m->name,
+                m->type ? "map" : "flow", modelType);
+  if (m->type != 0 && isQr)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "map model %s: the QR method has no map branch", m->name);
   if (dimension != m->dim || paramsDim != m->nparams)
     return fail(CHAOS_LYAP_EINVAL, "model %s has dim %d and %d params (got %d, %d)", m->name,
                 m->dim, m->nparams, dimension, paramsDim);

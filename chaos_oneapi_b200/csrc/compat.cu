@@ -68,6 +68,14 @@ __device__ __forceinline__ void dverk(double *val, const F &fn, double step) {
                               264. / 1955. * k5[j] + 125. / 11592. * k7[j] + 43. / 616. * k8[j]);
 }
 
+// One map iteration, cuda/tools/mapstep.dp.cpp:6-19: val <- fn(val) through
+// a scratch copy (StepMAP for the state, StepMAPVAR for a tangent vector).
+template <int D, class F> __device__ __forceinline__ void map_step(double *val, const F &fn) {
+  double arg[D];
+  fn(val, arg);
+  for (int j = 0; j < D; j++) val[j] = arg[j];
+}
+
 template <int N> __device__ __forceinline__ double dot_seq(const double *a, const double *b) {
   double r = 0;
   for (int i = 0; i < N; i++) r += a[i] * b[i];
@@ -98,6 +106,84 @@ __device__ __forceinline__ void normalize_vecs(double (&v)[KM][N], int k, double
     double nr = sqrt(dot_seq<N>(v[i], v[i]));
     for (int q = 0; q < N; q++) v[i][q] = (v[i][q] / nr) * eps;
   }
+}
+
+// cuda/lyapunov.dp.cpp:182-225 (map branch): every iteration renormalises
+// and adds its log-norms; the loop counters are doubles stepped by 1.
+template <class M, int KM>
+__device__ void point_var_map(const CompatArgs &a, const double *p, double *x,
+                              double (&V)[KM][M::N], double *lyap, int k) {
+  constexpr int N = M::N;
+  DState<M> fs{p};
+  DVar<M> fv{p, x};
+  for (double t = 0; t < a.t_skip; t += 1) map_step<N>(x, fs);
+  for (int i = 0; i < KM; i++)
+    for (int q = 0; q < N; q++) V[i][q] = 0.;
+  for (int i = 0; i < KM; i++)
+    if (i < k) V[i][i] += a.eps;
+  for (double t = 0; t < a.t_skip_clp; t += 1) {
+    for (int i = 0; i < KM; i++)
+      if (i < k) map_step<N>(V[i], fv);
+    map_step<N>(x, fs);
+    ort_vecs<N, KM>(V, k);
+    normalize_vecs<N, KM>(V, k, a.eps);
+  }
+  for (double t = 0; t < a.calc_time; t += 1) {
+    for (int i = 0; i < KM; i++)
+      if (i < k) map_step<N>(V[i], fv);
+    map_step<N>(x, fs);
+    ort_vecs<N, KM>(V, k);
+    for (int i = 0; i < KM; i++)
+      if (i < k) lyap[i] += log(sqrt(dot_seq<N>(V[i], V[i])) / a.eps);
+    normalize_vecs<N, KM>(V, k, a.eps);
+  }
+  for (int i = 0; i < KM; i++)
+    if (i < k) lyap[i] = lyap[i] / a.calc_time;
+}
+
+// cuda/lyapunov.dp.cpp:70-128 (map branch): perturbed copies iterated beside
+// the state; the loop counters are int32_t compared with the double times.
+template <class M, int KM>
+__device__ void point_fd_map(const CompatArgs &a, const double *p, double *x,
+                             double (&S)[KM][M::N], double *lyap, int k) {
+  constexpr int N = M::N;
+  DState<M> fs{p};
+  for (int32_t t = 0; t < a.t_skip; t++) map_step<N>(x, fs);
+  for (int i = 0; i < KM; i++)
+    if (i < k) {
+      for (int q = 0; q < N; q++) S[i][q] = x[q];
+      S[i][i] += a.eps;
+    }
+  for (int32_t t = 0; t < a.t_skip_clp; t++) {
+    map_step<N>(x, fs);
+    for (int i = 0; i < KM; i++)
+      if (i < k) {
+        map_step<N>(S[i], fs);
+        for (int q = 0; q < N; q++) S[i][q] -= x[q];
+      }
+    ort_vecs<N, KM>(S, k);
+    normalize_vecs<N, KM>(S, k, a.eps);
+    for (int i = 0; i < KM; i++)
+      if (i < k)
+        for (int q = 0; q < N; q++) S[i][q] += x[q];
+  }
+  for (int32_t t = 0; t < a.calc_time; t++) {
+    map_step<N>(x, fs);
+    for (int i = 0; i < KM; i++)
+      if (i < k) map_step<N>(S[i], fs);
+    for (int i = 0; i < KM; i++)
+      if (i < k)
+        for (int q = 0; q < N; q++) S[i][q] -= x[q];
+    ort_vecs<N, KM>(S, k);
+    for (int i = 0; i < KM; i++)
+      if (i < k) lyap[i] += log(sqrt(dot_seq<N>(S[i], S[i])) / a.eps);
+    normalize_vecs<N, KM>(S, k, a.eps);
+    for (int i = 0; i < KM; i++)
+      if (i < k)
+        for (int q = 0; q < N; q++) S[i][q] += x[q];
+  }
+  for (int i = 0; i < KM; i++)
+    if (i < k) lyap[i] = lyap[i] / a.calc_time;
 }
 
 // cuda/lyapunov.dp.cpp:133-180, 224-225 (flow branch)
@@ -243,7 +329,14 @@ __global__ void __launch_bounds__(128) compat_kernel(const CompatArgs a) {
     lyap[i] = (a.accumulate && i < k) ? a.lyap.base[pt * a.lyap.ps + i * a.lyap.cs] : 0.;
 
   double V[KM][N];
-  if (a.method == 2) {
+  if constexpr (IsMap<M>::value) {  // FD or VAR (the reference's QR has no map branch)
+    if (a.method == 1) point_var_map<M, KM>(a, p, x, V, lyap, k);
+    else point_fd_map<M, KM>(a, p, x, V, lyap, k);
+    if (a.close)
+      for (int i = 0; i < KM; i++)
+        if (i < k)
+          for (int q = 0; q < N; q++) a.close[(pt * k + i) * N + q] = V[i][q];
+  } else if (a.method == 2) {
     point_qr<M>(a, p, x, lyap);
   } else {
     if (a.method == 1) point_var<M, KM>(a, p, x, V, lyap, k);
@@ -276,7 +369,9 @@ int launch_model(const CompatArgs &a, int block, cudaStream_t s) {
     switch (a.k) {
       case 1: return launch_one<M, 1>(a, block, s);
       case 2: return launch_one<M, 2>(a, block, s);
-      case 3: return launch_one<M, 3>(a, block, s);
+      case 3:
+        if constexpr (M::N >= 3) return launch_one<M, 3>(a, block, s);
+        return kErrUnsupported;
       case 4:
         if constexpr (M::N >= 4) return launch_one<M, 4>(a, block, s);
         return kErrUnsupported;
@@ -299,6 +394,7 @@ int launch_compat(int model, const CompatArgs &a, int block, cudaStream_t s) {
     case kChua: return launch_model<Chua>(a, block, s);
     case kHyperRossler: return launch_model<HyperRossler>(a, block, s);
     case kLorenz96: return launch_model<Lorenz96>(a, block, s);
+    case kHenon: return launch_model<Henon>(a, block, s);
     default: return kErrUnsupported;
   }
 }

@@ -26,8 +26,14 @@ enum ModelId : int32_t {
   kChua = 3,
   kHyperRossler = 4,
   kLorenz96 = 5,
-  kNumModels = 6
+  kHenon = 6,
+  kNumModels = 7
 };
+
+// Model type (model_factory.h ModelType): flows are integrated, maps
+// iterated (cuda/tools/mapstep.dp.cpp:6-19: the new state is f(state), the
+// new tangent vector J(state) v).  Flows are the default.
+template <class M> struct IsMap { static constexpr bool value = false; };
 
 // Shimizu-Morioka: x' = y, y' = -a y - x z + x, z' = -l z + x^2 ; p = (alpha, lamda)
 struct Shimizu {
@@ -139,5 +145,24 @@ struct Lorenz96 {
   template <class T> CL_HD static void jq_col(const T *q, T *dq, const T *p, const T *x) { jv(q, dq, p, x); }
   static constexpr int kFlopsF = 5 * N, kFlopsJv = 8 * N;
 };
+
+// Henon map: x -> 1 - a x^2 + y, y -> b x ; p = (a, b).  A map-type model
+// (the reference registers none; its configuration lists map entries and its
+// method code has map branches, cuda/lyapunov.dp.cpp:70-125,182-222).
+// lambda_1 + lambda_2 = ln |b| (det J = -b).
+struct Henon {
+  static constexpr int N = 2, NP = 2, ID = kHenon;
+  template <class T> CL_HD static void f(const T *x, T *dx, const T *p) {
+    dx[0] = T(1.0) - p[0] * x[0] * x[0] + x[1];
+    dx[1] = p[1] * x[0];
+  }
+  template <class T> CL_HD static void jv(const T *v, T *dv, const T *p, const T *x) {
+    dv[0] = T(-2.0) * p[0] * x[0] * v[0] + v[1];
+    dv[1] = p[1] * v[0];
+  }
+  template <class T> CL_HD static void jq_col(const T *q, T *dq, const T *p, const T *x) { jv(q, dq, p, x); }
+  static constexpr int kFlopsF = 6, kFlopsJv = 6;
+};
+template <> struct IsMap<Henon> { static constexpr bool value = true; };
 
 }  // namespace chaos

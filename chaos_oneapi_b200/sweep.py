@@ -216,14 +216,15 @@ class Sweep:
 
 def cuda_lyapunov(task_num, is_qr, is_var, inits, close_points, dimension, model, params,
                   params_dim, eps, step, lyap_exps, exps_num, time_skip, time_skip_clp,
-                  calc_time, add_skip_steps, stream=None, bn=32, bs=32):
+                  calc_time, add_skip_steps, stream=None, bn=32, bs=32, model_type=0):
     """The reference launcher's drop-in (chaos_lyap_cudaLyapunov) on torch
-    CUDA tensors.  Enqueued on torch's current stream when stream is None."""
+    CUDA tensors.  Enqueued on torch's current stream when stream is None.
+    model_type: 0 flow, 1 map (the named model's type)."""
     import torch
     if stream is None:
         stream = torch.cuda.current_stream().cuda_stream
     check(lib.chaos_lyap_cudaLyapunov(
-        bn, bs, task_num, int(is_qr), int(is_var), 0, _tptr(inits, "float64"),
+        bn, bs, task_num, int(is_qr), int(is_var), int(model_type), _tptr(inits, "float64"),
         _tptr(close_points, "float64") if close_points is not None else None, dimension,
         model.encode(), _tptr(params, "float64"), params_dim, eps, step,
         _tptr(lyap_exps, "float64"), exps_num, time_skip, time_skip_clp, calc_time,

@@ -93,7 +93,10 @@ enum {
  * reference's LyapunovParameters (tool_params.h:23-44): eps = epsilon,
  * h = integration_step, t_transient = skip_time_attractor, t_align =
  * skip_time_slave_trajectory, dt_renorm = skip_time_normalization, t_avg =
- * total_time, k = lyapunov_exponent_num, method = using_qr / using_var. */
+ * total_time, k = lyapunov_exponent_num, method = using_qr / using_var.
+ * Map models (type 1) take compat precision and FD or VAR; their times are
+ * iteration counts and they renormalise every iteration, as the reference's
+ * map branches do (cuda/lyapunov.dp.cpp:70-125,182-222). */
 typedef struct chaos_lyap_desc {
   int32_t struct_size;      /* sizeof(chaos_lyap_desc) */
   char model[32];           /* registered model name, e.g. "lorenz" */
@@ -237,7 +240,11 @@ int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);
  *     cuda/lyapunov.dp.cpp:331-332);
  *   - lyapExps is accumulated into, exactly like the reference
  *     (cuda/lyapunov.dp.cpp:169,253): zero it for a plain result;
- *   - inits and closePoints are written like the reference writes them.
+ *   - inits and closePoints are written like the reference writes them;
+ *   - modelType (0 flow, 1 map) must be the named model's type; maps run the
+ *     reference's FD / VAR map branches (cuda/lyapunov.dp.cpp:70-125,
+ *     182-222), and QR on a map is rejected (the reference has no QR map
+ *     branch).
  * Arithmetic is the compat FP64 form (bit-identical trajectories).
  * Enqueued on `stream`; returns after the launch. */
 int chaos_lyap_cudaLyapunov(int bn, int bs, size_t taskNum, int isQr, int isVar, int modelType,

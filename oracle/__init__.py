@@ -22,7 +22,8 @@ REF_PATH = os.path.join(HERE, "_ref", "libchaos_ref.so")
 REF_MAIN = os.path.join(HERE, "_ref", "chaos_ref_main")
 REF_TREE = "/root/reference"
 
-MODELS = {"shimizu": 0, "lorenz": 1, "rossler": 2, "chua": 3, "hyper_rossler": 4, "lorenz96": 5}
+MODELS = {"shimizu": 0, "lorenz": 1, "rossler": 2, "chua": 3, "hyper_rossler": 4, "lorenz96": 5,
+          "henon": 6}
 METHODS = {"fd": 0, "var": 1, "qr": 2}
 
 _D = ctypes.POINTER(ctypes.c_double)

@@ -30,13 +30,14 @@
 static int l96w(int i) { return (i + L96_N) % L96_N; }
 
 int orc_model_dim(int model) {
-  static const int d[ORC_NMODELS] = {3, 3, 3, 3, 4, L96_N};
+  static const int d[ORC_NMODELS] = {3, 3, 3, 3, 4, L96_N, 2};
   return (model >= 0 && model < ORC_NMODELS) ? d[model] : -1;
 }
 int orc_model_nparams(int model) {
-  static const int m[ORC_NMODELS] = {2, 3, 3, 4, 2, 2};
+  static const int m[ORC_NMODELS] = {2, 3, 3, 4, 2, 2, 2};
   return (model >= 0 && model < ORC_NMODELS) ? m[model] : -1;
 }
+int orc_model_is_map(int model) { return model == ORC_HENON; }
 
 static void model_f(int model, const double *x, double *dx, const double *p) {
   switch (model) {
@@ -70,6 +71,10 @@ static void model_f(int model, const double *x, double *dx, const double *p) {
     case ORC_LORENZ96:
       for (int i = 0; i < L96_N; ++i)
         dx[i] = (x[l96w(i + 1)] - x[l96w(i - 2)]) * x[l96w(i - 1)] - p[1] * x[i] + p[0];
+      break;
+    case ORC_HENON: /* map: dx is the next state */
+      dx[0] = 1.0 - p[0] * x[0] * x[0] + x[1];
+      dx[1] = p[1] * x[0];
       break;
   }
 }
@@ -108,6 +113,10 @@ static void model_var(int model, const double *v, double *dv, const double *p, c
       for (int i = 0; i < L96_N; ++i)
         dv[i] = (v[l96w(i + 1)] - v[l96w(i - 2)]) * x[l96w(i - 1)] +
                 (x[l96w(i + 1)] - x[l96w(i - 2)]) * v[l96w(i - 1)] - p[1] * v[i];
+      break;
+    case ORC_HENON:
+      dv[0] = -2.0 * p[0] * x[0] * v[0] + v[1];
+      dv[1] = p[1] * v[0];
       break;
   }
 }
@@ -325,6 +334,78 @@ static void point_fd(const fixed_cfg *c, const double *p, double *x, double *lya
   for (int i = 0; i < k; i++) lyap[i] = lyap[i] / c->calc_time;
 }
 
+/* One map iteration through a scratch copy: cuda/tools/mapstep.dp.cpp:6-11
+ * (StepMAP, ctx kind 0) and :13-19 (StepMAPVAR, kind 1). */
+static void map_step(double *val, int n, const deriv_ctx *c) {
+  double arg[L96_N];
+  deriv(c, val, arg);
+  for (int j = 0; j < n; j++) val[j] = arg[j];
+}
+
+/* cuda/lyapunov.dp.cpp:182-225: VAR map branch (double counters stepped by
+ * 1, Gram-Schmidt and log-norms every iteration). */
+static void point_var_map(const fixed_cfg *c, const double *p, double *x, double *lyap) {
+  const int n = orc_model_dim(c->model), k = c->k;
+  double V[L96_N * L96_N], proj[L96_N];
+  deriv_ctx fs = {c->model, 0, p, 0}, fv = {c->model, 1, p, x};
+  double t;
+  memset(proj, 0, sizeof proj);
+  for (t = 0; t < c->t_skip; t += 1) map_step(x, n, &fs);
+  memset(V, 0, sizeof(double) * k * n);
+  for (int i = 0; i < k; i++) V[i * n + i] += c->eps;
+  for (t = 0; t < c->t_skip_clp; t += 1) {
+    for (int i = 0; i < k; i++) map_step(&V[i * n], n, &fv);
+    map_step(x, n, &fs);
+    ort_vecs(V, n, k, proj);
+    normalize_vecs(V, n, k, c->eps);
+  }
+  for (t = 0; t < c->calc_time; t += 1) {
+    for (int i = 0; i < k; i++) map_step(&V[i * n], n, &fv);
+    map_step(x, n, &fs);
+    ort_vecs(V, n, k, proj);
+    for (int i = 0; i < k; i++) lyap[i] += log(norm_seq(&V[i * n], n) / c->eps);
+    normalize_vecs(V, n, k, c->eps);
+  }
+  for (int i = 0; i < k; i++) lyap[i] = lyap[i] / c->calc_time;
+}
+
+/* cuda/lyapunov.dp.cpp:70-128: FD map branch (int32_t counters compared
+ * with the double times, renormalisation every iteration). */
+static void point_fd_map(const fixed_cfg *c, const double *p, double *x, double *lyap) {
+  const int n = orc_model_dim(c->model), k = c->k;
+  double S[L96_N * L96_N], proj[L96_N];
+  deriv_ctx fs = {c->model, 0, p, 0};
+  memset(proj, 0, sizeof proj);
+  for (int32_t t = 0; t < c->t_skip; t++) map_step(x, n, &fs);
+  for (int i = 0; i < k; i++) {
+    memcpy(&S[i * n], x, sizeof(double) * n);
+    S[i * n + i] += c->eps;
+  }
+  for (int32_t t = 0; t < c->t_skip_clp; t++) {
+    map_step(x, n, &fs);
+    for (int i = 0; i < k; i++) {
+      map_step(&S[i * n], n, &fs);
+      for (int j = 0; j < n; j++) S[i * n + j] -= x[j];
+    }
+    ort_vecs(S, n, k, proj);
+    normalize_vecs(S, n, k, c->eps);
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < n; j++) S[i * n + j] += x[j];
+  }
+  for (int32_t t = 0; t < c->calc_time; t++) {
+    map_step(x, n, &fs);
+    for (int i = 0; i < k; i++) map_step(&S[i * n], n, &fs);
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < n; j++) S[i * n + j] -= x[j];
+    ort_vecs(S, n, k, proj);
+    for (int i = 0; i < k; i++) lyap[i] += log(norm_seq(&S[i * n], n) / c->eps);
+    normalize_vecs(S, n, k, c->eps);
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < n; j++) S[i * n + j] += x[j];
+  }
+  for (int i = 0; i < k; i++) lyap[i] = lyap[i] / c->calc_time;
+}
+
 static void point_qr(const fixed_cfg *c, const double *p, double *x, double *lyap) {
   const int n = orc_model_dim(c->model), nn = n * n;
   double *Q = malloc(sizeof(double) * nn * 12 + sizeof(double) * n);
@@ -397,7 +478,10 @@ static void fixed_point(void *a, int64_t i) {
   const double *p = j->params + i * j->m;
   double *x = j->inits + i * j->n, *o = j->out + i * j->c.k;
   for (int q = 0; q < j->c.k; q++) o[q] = 0;
-  if (j->c.method == ORC_VAR) point_var(&j->c, p, x, o);
+  if (orc_model_is_map(j->c.model)) {
+    if (j->c.method == ORC_VAR) point_var_map(&j->c, p, x, o);
+    else point_fd_map(&j->c, p, x, o);
+  } else if (j->c.method == ORC_VAR) point_var(&j->c, p, x, o);
   else if (j->c.method == ORC_FD) point_fd(&j->c, p, x, o);
   else point_qr(&j->c, p, x, o);
 }
@@ -407,7 +491,7 @@ int orc_lyap_fixed(int model, int method, int64_t P, const double *params, doubl
                    double calc_time, double add_skip_steps, double *out, int threads) {
   const int n = orc_model_dim(model);
   if (n < 0 || P < 0 || k < 1 || k > n || !(h > 0)) return -1;
-  if (method == ORC_QR && k != n) return -1;
+  if (method == ORC_QR && (k != n || orc_model_is_map(model))) return -1;
   if (method < ORC_FD || method > ORC_QR) return -1;
   fixed_job j = {{model, method, k, eps, h, t_skip, t_skip_clp, calc_time, add_skip_steps},
                  orc_model_nparams(model), n, params, inits, out};
@@ -660,6 +744,7 @@ int orc_lyap_adaptive(const orc_adaptive_cfg *cfg, int64_t P, const double *para
   const int n = orc_model_dim(cfg->model);
   if (n < 0 || P < 0 || cfg->k < 1 || cfg->k > n || !(cfg->dt_renorm > 0) || !(cfg->t_avg > 0))
     return -1;
+  if (orc_model_is_map(cfg->model)) return -1; /* maps are iterated, not integrated */
   adapt_job j = {cfg, orc_model_nparams(cfg->model), n, params, inits, out, status, steps};
   run_parallel(P, threads, adaptive_point, &j);
   return 0;

@@ -18,19 +18,22 @@ extern "C" {
 #endif
 
 enum { ORC_SHIMIZU = 0, ORC_LORENZ = 1, ORC_ROSSLER = 2, ORC_CHUA = 3, ORC_HYPER_ROSSLER = 4,
-       ORC_LORENZ96 = 5, ORC_NMODELS = 6 };
+       ORC_LORENZ96 = 5, ORC_HENON = 6, ORC_NMODELS = 7 };
 enum { ORC_FD = 0, ORC_VAR = 1, ORC_QR = 2 };
 enum { ORC_DVERK65 = 0, ORC_DOPRI5 = 1 };
 enum { ORC_CGS = 0, ORC_MGS = 1 };
 
 int orc_model_dim(int model);
 int orc_model_nparams(int model);
+/* 1 for map-type models (iterated: cuda/tools/mapstep.dp.cpp:6-19). */
+int orc_model_is_map(int model);
 
 /* One fixed DVERK step of the state, in the reference's operation order
  * (cuda/tools/dverk.dp.cpp:7-43). */
 void orc_dverk_step(int model, double *x, const double *p, double h);
 
-/* Fixed-step reference methods (cuda/lyapunov.dp.cpp:5-259), flow models.
+/* Fixed-step reference methods (cuda/lyapunov.dp.cpp:5-259); map models take
+ * the FD / VAR map branches (:70-125, :182-222; no QR).
  * params P*m and inits P*n are point-major; inits are advanced in place to the
  * end states; out is P*k.  Returns 0, or -1 on bad arguments. */
 int orc_lyap_fixed(int model, int method, int64_t P, const double *params, double *inits,

@@ -1,4 +1,4 @@
-// Test infrastructure only (oracle build): extra flow models written in the
+// Test infrastructure only (oracle build): extra models written in the
 // reference's own model-plugin format so that the reference's Lyapunov path
 // (cuda/lyapunov.dp.cpp) can be run on them as the parity oracle.  The
 // reference ships only Shimizu-Morioka (cuda/models/flows/shimizu.dp.cpp);
@@ -89,6 +89,18 @@ void lorenz96_var(const double *v, double *dv, const double *p, const double *x)
             (x[wrap(i + 1)] - x[wrap(i - 2)]) * v[wrap(i - 1)] - p[1] * v[i];
 }
 
+// ------------------------------------------------------------ Henon map
+// x -> 1 - a x^2 + y, y -> b x ; p = (a, b).  A map-type model: f writes the
+// next state (cuda/tools/mapstep.dp.cpp:6-11), f_var the tangent image J(x) v.
+void henon(const double *x, double *dx, const double *p) {
+  dx[0] = 1.0 - p[0] * x[0] * x[0] + x[1];
+  dx[1] = p[1] * x[0];
+}
+void henon_var(const double *v, double *dv, const double *p, const double *x) {
+  dv[0] = -2.0 * p[0] * x[0] * v[0] + v[1];
+  dv[1] = p[1] * v[0];
+}
+
 // J*Q for a row-major n*n Q: column c of the result is J applied to column c
 // of Q, evaluated with the model's own tangent expression.
 template <int N, void (*VAR)(const double *, double *, const double *, const double *)>
@@ -101,13 +113,13 @@ void linear_q(const double *Q, double *res, const double *p, const double *x) {
   }
 }
 
-template <diffSysFunc F, diffSysFuncVar V, diffSysFuncVar Q>
+template <diffSysFunc F, diffSysFuncVar V, diffSysFuncVar Q, ModelType TYPE = ModelType::flow>
 struct Registrar : public ModelFactoryRegistry {
   Registrar(const char *name, int dim, int np, const char *pnames, const char *phase, const char *eq) {
     auto f = [](diffSysFunc *out) { *out = F; };
     auto fv = [](diffSysFuncVar *out) { *out = V; };
     auto fq = [](diffSysFuncVar *out) { *out = Q; };
-    RegisterModel(name, dim, np, ModelType::flow, f, fv, nullptr, nullptr, fq, pnames, phase, eq);
+    RegisterModel(name, dim, np, TYPE, f, fv, nullptr, nullptr, fq, pnames, phase, eq);
   }
 };
 
@@ -123,6 +135,8 @@ Registrar<chua, chua_var, linear_q<3, chua_var>> reg_chua(
 Registrar<hyper_rossler, hyper_rossler_var, linear_q<4, hyper_rossler_var>> reg_hyper_rossler(
     "hyper_rossler", 4, 2, "c, d", "x, y, z, w",
     "x' = - y - z;y' = x + 0.25 * y + w;z' = 3 + x * z;w' = - c * z + d * w");
+Registrar<henon, henon_var, linear_q<2, henon_var>, ModelType::map> reg_henon(
+    "henon", 2, 2, "a, b", "x, y", "x -> 1 - a * x^2 + y;y -> b * x");
 Registrar<lorenz96, lorenz96_var, linear_q<L96_N, lorenz96_var>> reg_lorenz96(
     "lorenz96", L96_N, 2, "F, gamma", "x0..x39",
     "x_i' = (x_{i+1} - x_{i-2}) * x_{i-1} - gamma * x_i + F (cyclic, N = 40)");

@@ -34,7 +34,10 @@ def test_desc_defaults_and_registry(lib):
     assert native.lib.chaos_lyap_abi_version() == 1
     names = lib.model_names()
     assert names == sorted(names)
-    assert {"shimizu", "lorenz", "rossler", "chua", "hyper_rossler", "lorenz96"} <= set(names)
+    assert {"shimizu", "lorenz", "rossler", "chua", "hyper_rossler", "lorenz96",
+            "henon"} <= set(names)
+    assert lib.model_info("henon")["type"] == "map"
+    assert lib.model_info("lorenz")["type"] == "flow"
     info = lib.model_info("shimizu")
     # the reference's own registration strings (shimizu.dp.cpp:204)
     assert info["dim"] == 3 and info["nparams"] == 2
@@ -52,6 +55,8 @@ def test_desc_defaults_and_registry(lib):
     (dict(method="fd", precision="fp64"), 3),                             # adaptive = VAR
     (dict(rtol=-1.0), 1),
     (dict(dt_renorm=0.0), 1),
+    (dict(model="henon", k=2), 3),                                        # maps: compat only
+    (dict(model="henon", k=2, method="qr", precision="compat", integrator="dverk"), 3),
 ])
 def test_descriptor_validation_precedes_device(lib, kw, code):
     cfg = dict(model="lorenz", t_avg=10.0, dt_renorm=1.0)

@@ -90,3 +90,60 @@ def test_compat_host_buffers_match_device(lib, orc):
     assert (status == 0).all()
     assert np.array_equal(x, want_x)
     np.testing.assert_allclose(spec, want, rtol=0, atol=1e-12)
+
+
+# Map-type model (Henon): the reference's FD / VAR map branches; times are
+# iteration counts.
+MAP_CASE = ([1.3, 0.3], [0.1, 0.1], 2, 1.0, 100.0, 50.0, 500.0, 1.0)
+
+
+@pytest.mark.parametrize("method", ["fd", "var"])
+@pytest.mark.parametrize("k", [1, 2])
+def test_compat_map_bitwise(lib, orc, method, k):
+    import torch
+    pb, xb, _, h, ts, tc, tt, dn = MAP_CASE
+    P = 37
+    rng = np.random.default_rng(5)
+    params = np.array(pb)[None, :] * (1 + 0.02 * rng.uniform(-1, 1, (P, 2)))
+    inits = orc.make_inits(2, P, xb, 1e-3, 0, 5)
+    want, want_x = orc.fixed("henon", method, params, inits, 1e-7, h, k, ts, tc, tt, dn / h)
+    sw = lib.Sweep(model="henon", method=method, integrator="dverk", precision="compat", k=k,
+                   eps=1e-7, h=h, t_transient=ts, t_align=tc, t_avg=tt, dt_renorm=dn)
+    dp = torch.from_numpy(params).cuda()
+    dx = torch.from_numpy(inits).cuda()
+    ds = torch.zeros((P, k), dtype=torch.float64, device="cuda")
+    st = torch.full((P,), -1, dtype=torch.int32, device="cuda")
+    sw.run(dp, dx, ds, st)
+    sw.sync()
+    assert (st.cpu().numpy() == 0).all()
+    assert np.array_equal(dx.cpu().numpy(), want_x), "end states differ"
+    np.testing.assert_allclose(ds.cpu().numpy(), want, rtol=0, atol=1e-12)
+    if k == 2 and method == "var":  # det J = -b: lambda_1 + lambda_2 = ln b
+        got = ds.cpu().numpy()
+        np.testing.assert_allclose(got.sum(1), np.log(params[:, 1]), rtol=0, atol=1e-12)
+
+
+def test_cuda_lyapunov_dropin_map(lib, orc):
+    """The launcher drop-in with modelType = map runs the map branch; a flow
+    model passed as a map (or the QR method on a map) is refused."""
+    import torch
+    pb, xb, k, h, ts, tc, tt, dn = MAP_CASE
+    P = 5
+    params = np.tile(pb, (P, 1))
+    inits = orc.make_inits(2, P, xb, 1e-3, 0, 9)
+    want, want_x = orc.fixed("henon", "fd", params, inits, 1e-7, h, k, ts, tc, tt, dn / h)
+    dp = torch.from_numpy(params).cuda()
+    dx = torch.from_numpy(inits).cuda()
+    out = torch.zeros((P, k), dtype=torch.float64, device="cuda")
+    close = torch.zeros((P * k * 2,), dtype=torch.float64, device="cuda")
+    lib.cuda_lyapunov(P, False, False, dx, close, 2, "henon", dp, 2, 1e-7, h, out, k, ts, tc, tt,
+                      dn / h, model_type=1)
+    torch.cuda.synchronize()
+    assert np.array_equal(dx.cpu().numpy(), want_x)
+    np.testing.assert_allclose(out.cpu().numpy(), want, rtol=0, atol=1e-12)
+    with pytest.raises(lib.ChaosError):
+        lib.cuda_lyapunov(P, False, False, dx, close, 2, "henon", dp, 2, 1e-7, h, out, k, ts, tc,
+                          tt, dn / h, model_type=0)
+    with pytest.raises(lib.ChaosError):
+        lib.cuda_lyapunov(P, True, False, dx, close, 2, "henon", dp, 2, 1e-7, h, out, k, ts, tc,
+                          tt, dn / h, model_type=1)

@@ -50,6 +50,34 @@ def test_restatement_matches_live_reference_bitwise(orc, model, k, method):
     assert np.array_equal(a[1], b[1]) and np.array_equal(a[0], b[0])
 
 
+@pytest.mark.skipif(not __import__("oracle").have_ref(), reason="reference build not present")
+@pytest.mark.parametrize("method", ["fd", "var"])
+@pytest.mark.parametrize("k", [1, 2])
+def test_map_branches_match_live_reference_bitwise(orc, method, k):
+    """A map-type model (Henon, registered as ModelType::map in the oracle
+    build) through the reference's map branches (cuda/lyapunov.dp.cpp:70-125,
+    182-222), including non-integer iteration counts (int32_t counters in FD,
+    double counters in VAR)."""
+    rng = np.random.default_rng(3)
+    P = 6
+    params = np.stack([rng.uniform(1.0, 1.4, P), rng.uniform(0.2, 0.3, P)], 1)
+    inits = np.array([0.1, 0.1])[None, :] + 1e-3 * rng.standard_normal((P, 2))
+    for ts, tc, tt in ((100.0, 50.0, 400.0), (10.5, 3.25, 40.5)):
+        a = orc.reference("henon", method, params, inits, 1e-7, 1.0, k, ts, tc, tt, 1.0, threads=2)
+        b = orc.fixed("henon", method, params, inits, 1e-7, 1.0, k, ts, tc, tt, 1.0, threads=2)
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[0], b[0])
+
+
+def test_map_trace_identity(orc):
+    """Henon: det J = -b, so lambda_1 + lambda_2 = ln b for any orbit."""
+    params = np.array([[1.4, 0.3], [1.2, 0.25]])
+    inits = np.array([[0.1, 0.1], [0.0, 0.2]])
+    spec, _ = orc.fixed("henon", "var", params, inits, 1e-7, 1.0, 2, 1000.0, 100.0, 20000.0, 1.0)
+    np.testing.assert_allclose(spec.sum(1), np.log(params[:, 1]), rtol=0, atol=1e-12)
+    # classic Henon (a = 1.4, b = 0.3): lambda_1 = 0.419 (published value)
+    assert abs(spec[0, 0] - 0.419) < 5e-3
+
+
 def test_reference_quirks_reproduced(orc):
     """Renormalisation fires on skipCount == addSkipSteps (a double compare):
     a non-integer ratio never fires, so no log-norm is ever accumulated."""
