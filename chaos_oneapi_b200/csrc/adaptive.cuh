@@ -711,7 +711,10 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
     L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
     const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
     const float dt = (float)a.dt_renorm;
-    L.L = fminf(dt, fmaxf(dt * (1.0f / kRenormSplitMax), target));
+    // Growth is limited to 2x per renormalisation: a calm stretch (the first
+    // interval of a phase, the slow part of an orbit) must not open an
+    // interval long enough to cross a contraction burst unrenormalised.
+    L.L = fminf(fminf(dt, 2.0f * L.L), fmaxf(dt * (1.0f / kRenormSplitMax), target));
   }
   L.t_gs = 0.f;
   refresh_tangent_derivs(L);

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
       const double rate = 0.5 * (double)logf((float)cancel) / w.t_gs;
       w.rate_max = fmax(rate, 0.995 * w.rate_max);
       const double target = 0.125 * tau / fmax(w.rate_max, 1e-30);
-      w.L = fmin(a.dt_renorm, fmax(a.dt_renorm / 64, target));
+      w.L = fmin(fmin(a.dt_renorm, 2.0 * w.L), fmax(a.dt_renorm / 64, target));  // grows <= 2x
     }
     w.t_gs = 0.0;
     refresh_kv(w, V, KV, k, g, li, left, right);

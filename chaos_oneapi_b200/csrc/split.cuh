@@ -256,7 +256,7 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
     L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
     const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
     const float dt = (float)a.dt_renorm;
-    L.L = fminf(dt, fmaxf(dt * (1.0f / kRenormSplitMax), target));
+    L.L = fminf(fminf(dt, 2.0f * L.L), fmaxf(dt * (1.0f / kRenormSplitMax), target));
   }
   L.t_gs = 0.f;
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
