@@ -263,7 +263,7 @@ def run_surrogate_bench(a, rank, world, local):
                   rtol=1e-10, atol=1e-10, h=1e-3, t_transient=100.0, t_avg=1000.0, dt_renorm=1.0,
                   device=local)
     P = n * n
-    rng = np.random.default_rng(2024)
+    rng = np.random.default_rng(a.held_out_seed)
     held = rng.choice(P, 10000, replace=False)
     truth, st = plain_sweep(sw, spec, held)
     sample = rng.choice(P, min(P, 1 << 18), replace=False)
@@ -272,7 +272,8 @@ def run_surrogate_bench(a, rank, world, local):
     plain_sweep(sw, spec, sample)
     plain_est = (time.perf_counter() - t0) * P / sample.size
     cfg = RefineConfig(steps0=6000, steps_round=4000, rounds=4, round_grid_step=max(1, n // 512),
-                       round_max_new=65536, rule=a.surrogate_rule)
+                       round_max_new=65536, rule=a.surrogate_rule,
+                       regime_conf=a.regime_conf, regime_std=a.regime_std)
     if cfg.rule == "regime":
         cfg.lam_limit = 0.005
         rule = (f"integrate where the ensemble's regime score r = tanh((lambda_1 - "
@@ -300,7 +301,8 @@ def run_surrogate_bench(a, rank, world, local):
     if cfg.rule == "regime":
         import torch
         from chaos_oneapi_b200.surrogate import _flags
-        for conf, sd in ((0.5, 0.2), (0.7, 0.15), (0.8, 0.1), (0.9, 0.05)):
+        for conf, sd in ((0.5, 0.2), (0.7, 0.15), (0.7, 0.1), (0.8, 0.15), (0.8, 0.12),
+                         (0.8, 0.1), (0.85, 0.1), (0.9, 0.05)):
             c2 = RefineConfig(**{**cfg.__dict__, "regime_conf": conf, "regime_std": sd,
                                  "timings": {}})
             fl = _flags(torch.from_numpy(pm), torch.from_numpy(ps), c2).numpy() | mask[held]
@@ -309,6 +311,9 @@ def run_surrogate_bench(a, rank, world, local):
                          "plain_fraction": float(fl.mean()),
                          "regime_agreement": float(((pred > 0.01) == (truth[:, 0] > 0.01))[ok]
                                                    .mean())})
+    if a.dump:
+        np.savez_compressed(a.dump, held=held, truth=truth, status=st, mean=pm, std=ps,
+                            plain=mask[held], out=out[held])
     if rank == 0:
         line = {
             "metric": METRIC + " (surrogate-refined map)", "value": P / refined, "unit": "points/s",
@@ -325,7 +330,8 @@ def run_surrogate_bench(a, rank, world, local):
             "refined_over_plain": refined / plain_est,
             "plain_fraction": info["plain_fraction"], "training_cells": info["training_cells"],
             "timings": info["timings"], "clocks": clk,
-            "held_out": {"cells": int(ok.sum()), "regime_agreement": agree,
+            "held_out": {"cells": int(ok.sum()), "seed": a.held_out_seed,
+                         "regime_agreement": agree,
                          "surrogate_filled": int(filled.sum()),
                          "median_abs_err_filled": ([float(x) for x in np.median(d[filled], 0)]
                                                    if filled.any() else None),
@@ -517,6 +523,14 @@ def main():
                          "(whose stiff points set the run's length) split, the others per lane")
     ap.add_argument("--surrogate-rule", default="regime", choices=["regime", "spread"],
                     help="surrogate: which cells the plain sweep integrates (see RefineConfig)")
+    ap.add_argument("--regime-conf", type=float, default=0.7,
+                    help="surrogate, regime rule: integrate where |mean r| is below this")
+    ap.add_argument("--regime-std", type=float, default=0.15,
+                    help="surrogate, regime rule: integrate where std r is above this")
+    ap.add_argument("--held-out-seed", type=int, default=2024,
+                    help="surrogate: seed of the 10,000 held-out cells")
+    ap.add_argument("--dump", default="",
+                    help="surrogate: write the held-out cells' predictions and truth (npz)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--accuracy-sample", type=int, default=256)
     ap.add_argument("--variant", type=int, default=-1,
