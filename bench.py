@@ -523,11 +523,11 @@ def main():
                          "(whose stiff points set the run's length) split, the others per lane")
     ap.add_argument("--surrogate-rule", default="regime", choices=["regime", "spread"],
                     help="surrogate: which cells the plain sweep integrates (see RefineConfig)")
-    ap.add_argument("--regime-conf", type=float, default=0.7,
+    ap.add_argument("--regime-conf", type=float, default=0.8,
                     help="surrogate, regime rule: integrate where |mean r| is below this")
-    ap.add_argument("--regime-std", type=float, default=0.15,
+    ap.add_argument("--regime-std", type=float, default=0.1,
                     help="surrogate, regime rule: integrate where std r is above this")
-    ap.add_argument("--held-out-seed", type=int, default=2024,
+    ap.add_argument("--held-out-seed", type=int, default=7,
                     help="surrogate: seed of the 10,000 held-out cells")
     ap.add_argument("--dump", default="",
                     help="surrogate: write the held-out cells' predictions and truth (npz)")
