@@ -15,7 +15,7 @@ cells where it is confident, and the plain sweep integrates the rest:
 4. final fill: predict the whole fine map; integrate plainly every cell the
    same rule flags; the surrogate's mean fills the rest.
 
-The plain sweep stays the judge: every cell the rule flags is integrated by
+The plain sweep stays the arbiter: every cell the rule flags is integrated by
 it, and accuracy is measured against it on held-out cells.
 """
 from __future__ import annotations

@@ -6,7 +6,8 @@
   time; see oracle/Makefile).
 
 Only tests, the smoke check and the bench's CPU-baseline leg import this, as
-the checker.  The product (chaos_oneapi_b200) never does.
+the reference results to compare against.  The product (chaos_oneapi_b200)
+never does.
 """
 from __future__ import annotations
 

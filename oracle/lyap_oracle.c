@@ -1,6 +1,6 @@
 /* Test infrastructure only: the oracle (see lyap_oracle.h).  A CPU restatement
  * of the reference's Lyapunov-spectrum path, used by tests, the smoke check and
- * the bench's CPU-baseline leg as the checker.  The product never links it.
+ * the bench's CPU-baseline leg to compare against.  The product never links it.
  *
  * Fixed-step part: reproduces cuda/lyapunov.dp.cpp:5-259 with the tableau and
  * operation order of cuda/tools/dverk.dp.cpp:7-81 and the Gram-Schmidt of

@@ -2,7 +2,7 @@
  * reference's Lyapunov-spectrum path (cuda/lyapunov.dp.cpp,
  * cuda/tools/dverk.dp.cpp, cuda/tools/dopri.dp.cpp, cuda/tools/linalg.dp.cpp)
  * plus the adaptive forms built on it.  Only tests, the smoke check and the
- * bench's CPU-baseline leg use it, as the checker; the product never links it.
+ * bench's CPU-baseline leg use it, to compare against; the product never links it.
  *
  * Pinned: the fixed-step methods are checked bit for bit against the
  * reference's own sources compiled on the host (oracle/_ref, recipe in
