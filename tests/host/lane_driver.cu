@@ -6,7 +6,8 @@
 // tests/test_host_lane.py with nvcc; never linked into the library.
 //
 //   lane_driver MODEL PREC INTEG rtol h0 t_transient t_align t_avg dt_renorm p0 p1 [p2 [p3]] -- x0 x1 ...
-//   MODEL: rossler | lorenz | chua | hyper_rossler; PREC: fp32 | fp64; INTEG: dopri5 | dverk65
+//   MODEL: rossler | lorenz | chua | hyper_rossler; PREC: fp32 | fp64;
+//   INTEG: dopri5 | dverk65, with the suffix "+mgs" for modified Gram-Schmidt
 // Prints: status steps lambda_1 ... lambda_n
 #include <cstdio>
 #include <cstdlib>
@@ -34,7 +35,8 @@ int main(int argc, char **argv) {
   if (argc < 12) return 2;
   const char *model = argv[1];
   const bool fp32 = !std::strcmp(argv[2], "fp32");
-  const bool dopri = !std::strcmp(argv[3], "dopri5");
+  const bool dopri = !std::strncmp(argv[3], "dopri5", 6);
+  const bool mgs = std::strstr(argv[3], "+mgs") != nullptr;
   std::vector<double> p, x;
   int i = 10;
   for (; i < argc && std::strcmp(argv[i], "--"); i++) p.push_back(std::atof(argv[i]));
@@ -46,7 +48,7 @@ int main(int argc, char **argv) {
   AdaptiveArgs a{};
   a.P = 1;
   a.k = n;
-  a.gs = 0;
+  a.gs = mgs ? 1 : 0;
   a.rtol = a.atol = std::atof(argv[4]);
   a.h0 = std::atof(argv[5]);
   a.t_transient = std::atof(argv[6]);

@@ -87,3 +87,19 @@ def test_lane_escape_status_matches_oracle(driver, orc):
                       1.0, p, x0)
     assert rst[0] == 4 and st == 4
     assert np.isnan(lam).all()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_lane_mgs_and_alignment_phase(driver, orc, prec):
+    """Modified Gram-Schmidt and an alignment phase (renormalised, not
+    accumulated) before the averaging window, against the oracle with the
+    same phases."""
+    model, p, x0, ts, tt, dt = CASES[0]
+    ta = 20.0
+    ref, rst, _ = orc.adaptive(model, np.array([p]), np.array([x0]), 3, integrator="dverk65",
+                               gs="mgs", rtol=1e-12, atol=1e-12, t_transient=ts, t_align=ta,
+                               t_avg=tt, dt_renorm=dt)
+    assert rst[0] == 0
+    st, _, lam = _run(driver, model, prec, "dopri5+mgs", 1e-6, 1e-2, ts, ta, tt, dt, p, x0)
+    assert st == 0
+    np.testing.assert_allclose(lam, ref[0], rtol=0, atol=1e-4)
