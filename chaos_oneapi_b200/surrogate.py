@@ -213,8 +213,8 @@ class RefineConfig:
     lam_limit: float = 0.05        # predicted |lambda_1| ("spread"); |lambda_1 - thr| ("regime")
     regime_threshold: float = 0.01
     regime_width: float = 0.005
-    regime_conf: float = 0.7
-    regime_std: float = 0.15
+    regime_conf: float = 0.8
+    regime_std: float = 0.1
     seed: int = 0
     timings: dict = field(default_factory=dict)
 
