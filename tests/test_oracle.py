@@ -114,6 +114,16 @@ def test_adaptive_oracle_lorenz_literature_values(orc):
     assert abs(out[0, 2] + 14.572) < 0.02
 
 
+def test_adaptive_oracle_rossler_literature_values(orc):
+    """Classic Rossler (0.2, 0.2, 5.7): lambda ~ (0.0714, 0, -5.394)."""
+    out, st, _ = orc.adaptive("rossler", np.array([[0.2, 0.2, 5.7]]), np.array([[1.0, 1.0, 0.0]]),
+                              3, rtol=1e-10, atol=1e-10, t_transient=500.0, t_avg=5000.0,
+                              dt_renorm=1.0)
+    assert st[0] == 0
+    assert abs(out[0, 0] - 0.0714) < 3e-3 and abs(out[0, 1]) < 2e-3
+    assert abs(out[0, 2] + 5.394) < 5e-3
+
+
 def test_philox_matches_numpy(orc):
     """Philox4x64-10 against numpy's independent implementation (numpy
     advances the counter before the first block)."""
