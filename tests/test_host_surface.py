@@ -102,3 +102,31 @@ def test_writer_matches_reference_program_bytewise(lib, orc, tmp_path):
     assert (out / "Lyapunov shimizu.json").read_bytes() == ref_json
     full = np.load(out / "Lyapunov shimizu.npy")
     assert full.shape == (12, 5) and np.array_equal(full[:, 2:], spec)
+
+
+def test_map_model_plan_and_writer(lib, orc, tmp_path):
+    """A map-type model through the host surface: the grid is planned like a
+    flow's, and the writer records systemType 1 (ModelType::map,
+    model_factory.h:22-25) beside the rows."""
+    cfg = json.loads(json.dumps(CFG))
+    cfg["systems"][0].update(model_name="henon", lyapunov_exponent_num=2, integration_step=1.0,
+                             skip_time_attractor=100, skip_time_slave_trajectory=50,
+                             skip_time_normalization=1, total_time=500,
+                             initial_state=[0.1, 0.1], initial_model_params=[1.3, 0.3],
+                             first_sweep_param=[0, 1.0, 1.4, 3], second_sweep_param=[1, 0.2, 0.3, 2])
+    p = tmp_path / "config.json"
+    p.write_text(json.dumps(cfg))
+    params, inits = _plan(lib, str(p), "henon")
+    assert np.array_equal(params, orc.make_grid(2, [1.3, 0.3], [0, 1.0, 1.4, 3], [1, 0.2, 0.3, 2]))
+    assert np.array_equal(inits, np.tile([0.1, 0.1], (6, 1)))
+    spec, _ = orc.fixed("henon", "var", params, inits, 1e-7, 1.0, 2, 100, 50, 500, 1.0)
+    so, D = _host(lib)
+    spec = np.ascontiguousarray(spec)
+    assert so.chaos_host_save(str(p).encode(), b"henon", spec.ctypes.data_as(D),
+                              str(tmp_path).encode()) == 0
+    out = json.loads((tmp_path / "Lyapunov henon.json").read_text())
+    assert out["Model"]["systemType"] == 1 and out["Model"]["Dimension"] == 2
+    rows = [r.split() for r in out["_Data"].strip().split("\n")]
+    assert len(rows) == 6 and all(len(r) == 4 for r in rows)
+    full = np.load(tmp_path / "Lyapunov henon.npy")
+    assert np.array_equal(full[:, 2:], spec)
