@@ -42,6 +42,7 @@ CUDA_UNITS = {
     "order.cu": [],
     "split.cu": [],
     "mlp.cu": [],
+    "trajectory.cu": [],
 }
 CXX_UNITS = ["inputs.cpp"]
 HOST_UNITS = ["model_factory.cpp", "tool_params.cpp", "task_lyapunov.cpp", "filehandler.cpp",

@@ -7,8 +7,10 @@
 //    error estimate; Dopri5 of cuda/tools/dopri.dp.cpp:14-44 (FSAL).
 //  * Step-size control: cuda/tools/dopri.dp.cpp:9-12,46-138 (safety 0.9,
 //    fac1 0.2, fac2 10, beta 0.04, exponent 1/q - 0.75 beta, error = RMS of
-//    e / (atol + rtol max(|y0|,|y1|)), reject / retry), evaluated in FP32
-//    (it only steers the step length).
+//    e / (atol + rtol max(|y0|,|y1|)), reject / retry).  The FP64 form
+//    evaluates the error norm and the controller in FP64, so that its step
+//    sequence follows the reference's dopriStep to rounding; the FP32 form in
+//    FP32 with fast reciprocals (there it only steers the step length).
 //  * Variational equations are integrated jointly with the state: within one
 //    step the state is advanced first and its stage points X_s are kept, then
 //    each tangent vector runs the same stages with J(X_s).  This is the same
@@ -24,6 +26,7 @@
 
 #include "kernels.h"
 #include "models.cuh"
+#include "renorm.cuh"
 
 namespace chaos {
 namespace adaptive {
@@ -63,28 +66,11 @@ struct DP {  // Dormand-Prince 5(4), FSAL
 
 template <class R> CL_HD R C(double v) { return R(v); }
 
-CL_HD float fast_log2f(float x) {
-#ifdef __CUDA_ARCH__
-  return __log2f(x);
-#else
-  return log2f(x);
-#endif
-}
 CL_HD double quiet_nan() {
 #ifdef __CUDA_ARCH__
   return __longlong_as_double(0x7ff8000000000000ULL);
 #else
   return __builtin_nan("");
-#endif
-}
-
-// Error weight contribution of one component (the error norm only steers the
-// step length, so an approximate reciprocal is enough).
-CL_HD float fast_div(float a, float b) {
-#ifdef __CUDA_ARCH__
-  return __fdividef(a, b);
-#else
-  return a / b;
 #endif
 }
 
@@ -144,15 +130,21 @@ CL_HD E lin(double c, E k, Rest... rest) {
   return lin_acc<S, E>(vmul(S(c), k), rest...);
 }
 
+// Arithmetic of the error norm and the step-size controller: FP32 for the
+// FP32 form, FP64 for the FP64 form.
+template <class R> struct CtlReal { using type = float; };
+template <> struct CtlReal<double> { using type = double; };
+
 // Squared weighted error e / (atol + rtol max(|y0|, |y1|)) accumulated per
-// row: a float accumulator for a scalar row, a float2 for a packed pair.
+// row: a float accumulator for a scalar FP32 row, a float2 for a packed pair,
+// a double for an FP64 row.
 template <class E> struct ErrAcc { using type = float; };
 template <> struct ErrAcc<float2> { using type = float2; };
+template <> struct ErrAcc<double> { using type = double; };
 
-template <class R>
-CL_HD void err_acc(R y0, R y1, R e, float rtol, float atol, float &acc) {
-  const float m = fmaxf(fabsf((float)y0), fabsf((float)y1));
-  const float r = fast_div((float)e, fmaf(rtol, m, atol));
+CL_HD void err_acc(float y0, float y1, float e, float rtol, float atol, float &acc) {
+  const float m = fmaxf(fabsf(y0), fabsf(y1));
+  const float r = fast_div(e, fmaf(rtol, m, atol));
   acc = fmaf(r, r, acc);
 }
 // The pair shares one reciprocal: 1 / (s_x s_y) scaled by the other weight.
@@ -163,13 +155,48 @@ CL_HD void err_acc(float2 y0, float2 y1, float2 e, float rtol, float atol, float
   const float2 r = vmul2(e, make_float2(sy * inv, sx * inv));
   acc = vfma2(r, r, acc);
 }
+CL_HD double recip(double x) {
+#ifdef __CUDA_ARCH__
+  return __drcp_rn(x);
+#else
+  return 1.0 / x;
+#endif
+}
+// Error terms of one row of N components; he = h e, the scaled error vector.
+// FP64 rows take their components in pairs sharing one correctly rounded
+// reciprocal of the product of their weights (a few ulp from the e / s of the
+// reference's division).
+template <int N, class E, class T, class A>
+CL_HD void err_row(const E *y0, const E *y1, const E *he, T rtol, T atol, A &acc) {
+  if constexpr (std::is_same<E, double>::value) {
+#pragma unroll
+    for (int j = 0; j + 1 < N; j += 2) {
+      const double sx = fma(rtol, fmax(fabs(y0[j]), fabs(y1[j])), atol);
+      const double sy = fma(rtol, fmax(fabs(y0[j + 1]), fabs(y1[j + 1])), atol);
+      const double inv = recip(sx * sy);
+      const double rx = he[j] * (sy * inv), ry = he[j + 1] * (sx * inv);
+      acc = fma(rx, rx, acc);
+      acc = fma(ry, ry, acc);
+    }
+    if (N % 2) {
+      const double sk = fma(rtol, fmax(fabs(y0[N - 1]), fabs(y1[N - 1])), atol);
+      const double r = he[N - 1] * recip(sk);
+      acc = fma(r, r, acc);
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < N; j++) err_acc(y0[j], y1[j], he[j], rtol, atol, acc);
+  }
+}
 
 // One DVERK 6(5) pass over an N-vector y of elements E: y1 = 6th-order
 // solution, err2 += squared weighted error components.  fn(s, arg, out)
 // evaluates the derivative of stage s (0-based) at arg.
 template <int N, class E, class F>
 CL_HD void dverk_pass(const E *y, typename ScalarOf<E>::type h, const F &fn, E *y1,
-                      typename ErrAcc<E>::type &err2, float rtol, float atol) {
+                      typename ErrAcc<E>::type &err2,
+                      typename CtlReal<typename ScalarOf<E>::type>::type rtol,
+                      typename CtlReal<typename ScalarOf<E>::type>::type atol) {
   using S = typename ScalarOf<E>::type;
   using T = DV;
   E k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
@@ -219,18 +246,20 @@ CL_HD void dverk_pass(const E *y, typename ScalarOf<E>::type h, const F &fn, E *
 #pragma unroll
     for (int j = 0; j < N; j++) {
       acc[j] = vfma(S(T::b8), k8[j], acc[j]);
-      e[j] = vfma(S(T::d8), k8[j], e[j]);
+      e[j] = vmul(h, vfma(S(T::d8), k8[j], e[j]));
       y1[j] = vfma(h, acc[j], y[j]);
-      err_acc(y[j], y1[j], vmul(h, e[j]), rtol, atol, err2);
     }
   }
+  err_row<N>(y, y1, e, rtol, atol, err2);
 }
 
 // One Dopri5 pass: k1 = derivative at y (FSAL, given), y1 = 5th-order
 // solution, k7 = derivative at y1 (the next step's k1).
 template <int N, class E, class F>
 CL_HD void dopri_pass(const E *y, const E *k1, typename ScalarOf<E>::type h, const F &fn,
-                      E *y1, E *k7, typename ErrAcc<E>::type &err2, float rtol, float atol) {
+                      E *y1, E *k7, typename ErrAcc<E>::type &err2,
+                      typename CtlReal<typename ScalarOf<E>::type>::type rtol,
+                      typename CtlReal<typename ScalarOf<E>::type>::type atol) {
   using S = typename ScalarOf<E>::type;
   using T = DP;
   E k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
@@ -266,10 +295,8 @@ CL_HD void dopri_pass(const E *y, const E *k1, typename ScalarOf<E>::type h, con
   }
   fn(6, y1, k7);
 #pragma unroll
-  for (int j = 0; j < N; j++) {
-    e[j] = vfma(S(T::e7), k7[j], e[j]);
-    err_acc(y[j], y1[j], vmul(h, e[j]), rtol, atol, err2);
-  }
+  for (int j = 0; j < N; j++) e[j] = vmul(h, vfma(S(T::e7), k7[j], e[j]));
+  err_row<N>(y, y1, e, rtol, atol, err2);
 }
 
 // Stage evaluators for the state pass (records stage points) and the tangent
@@ -299,15 +326,10 @@ struct TangentStages {
 enum Phase : int32_t { kTransient = 0, kAlign = 1, kAverage = 2 };
 enum LaneResult : int32_t { kRunning = 0, kFinished = 1 };
 
-constexpr int kRenormSplitInit = 16, kRenormSplitMax = 64;
 
-// Step-size controller constants (dopri.dp.cpp:9-12: safety 0.9, the step
-// may shrink by at most 1 / facc1 = 0.2 and grow by 1 / facc2 = 10, previous
-// error floored at 1e-4), as base-2 logarithms.
-constexpr float kLog2Safe = -0.15200309344504997f;   // log2 0.9
-constexpr float kLog2Facc1 = 2.321928094887362f;     // log2 5
-constexpr float kLog2Facc2 = -3.321928094887362f;    // log2 0.1
-constexpr float kLog2FacMin = -13.287712379549449f;  // log2 1e-4
+// log2 of the floor of the previous step's error (dopri.dp.cpp:65-68: 1e-4),
+// the controller's state at the start of an integration.
+template <class C> CL_HD C log2_fac_min() { return C(-13.287712379549449); }
 
 // Largest log of the Gram-Schmidt cancellation factor (|v_i| / r_i) allowed
 // between two renormalisations: 0.3 ln(1 / max(rtol, unit roundoff of R)).
@@ -318,10 +340,64 @@ template <class R> CL_HD float renorm_spread_limit(float rtol) {
 
 struct Ctl {
   float rtol, atol, tau;
+  double rtol64, atol64;  // the tolerances for the FP64 form's error norm
   double hmax, hmin;
   int64_t max_steps;
   double escape;
 };
+template <class R> CL_HD typename CtlReal<R>::type ctl_rtol(const Ctl &c) { return c.rtol; }
+template <> CL_HD double ctl_rtol<double>(const Ctl &c) { return c.rtol64; }
+template <class R> CL_HD typename CtlReal<R>::type ctl_atol(const Ctl &c) { return c.atol; }
+template <> CL_HD double ctl_atol<double>(const Ctl &c) { return c.atol64; }
+
+// Controller arithmetic of either precision: base-2 logarithm and power.
+CL_HD float ctl_log2(float x) { return fast_log2f(x); }
+CL_HD double ctl_log2(double x) { return log2(x); }
+CL_HD float ctl_exp2(float x) { return exp2f(x); }
+CL_HD double ctl_exp2(double x) { return exp2(x); }
+CL_HD float ctl_fma(float a, float b, float c) { return fmaf(a, b, c); }
+CL_HD double ctl_fma(double a, double b, double c) { return fma(a, b, c); }
+
+// Largest error mean square that counts as finite.
+template <class C> CL_HD C err2_limit() { return sizeof(C) == 4 ? C(3.4e38f) : C(1e300); }
+
+// The step-size controller of dopri.dp.cpp:46-138 after an attempted step of
+// length h with error mean square err2, in the log2 domain: with
+// l = log2 err, the reference's fac = err^expo1 facOld^-beta / safe clamped
+// to [facc2, facc1] = [0.1, 5] is lf = expo1 l - beta l_old - log2 safe
+// clamped to [log2 0.1, log2 5], and h_new = h 2^-lf.  Accepted (err <= 1):
+// returns true, hnew = the next proposal (at most hmax; after a rejection no
+// longer than h), lfac_old = max(l, log2 1e-4).  Rejected: returns false,
+// hnew = h / min(facc1, err^expo1 / safe).  R the state precision, C = its
+// controller precision (FP32 for FP32 states, FP64 for FP64 states).
+template <class R, int INTEG>
+CL_HD bool control(typename CtlReal<R>::type err2, R h, typename CtlReal<R>::type &lfac_old,
+                   bool &reject, double hmax, R &hnew) {
+  using C = typename CtlReal<R>::type;
+  constexpr C beta = C(0.04);
+  constexpr C expo1 = (INTEG == kDverk65 ? C(1.0 / 6.0) : C(0.2)) - beta * C(0.75);
+  constexpr C log2_safe = C(-0.15200309344504995);   // log2 0.9
+  constexpr C log2_facc1 = C(2.321928094887362);     // log2 5
+  constexpr C log2_facc2 = C(-3.321928094887362);    // log2 0.1
+  const C lerr = C(0.5) * ctl_log2(err2 > C(1e-38f) ? err2 : C(1e-38f));
+  if (err2 <= C(1)) {
+    C lf = ctl_fma(expo1, lerr, ctl_fma(-beta, lfac_old, -log2_safe));
+    lf = lf < log2_facc2 ? log2_facc2 : lf;
+    lf = lf < log2_facc1 ? lf : log2_facc1;
+    R hn = h * (R)ctl_exp2(-lf);
+    lfac_old = lerr > log2_fac_min<C>() ? lerr : log2_fac_min<C>();
+    if ((double)hn > hmax) hn = (R)hmax;
+    if (reject && hn > h) hn = h;
+    reject = false;
+    hnew = hn;
+    return true;
+  }
+  C lr = ctl_fma(expo1, lerr, -log2_safe);
+  lr = lr < log2_facc1 ? lr : log2_facc1;
+  hnew = h * (R)ctl_exp2(-lr);
+  reject = true;
+  return false;
+}
 
 // The whole integration state of one parameter point, owned by one lane.
 //
@@ -349,7 +425,7 @@ struct Lane {
   R kx[N];      // Dopri5 FSAL: derivative of the state
   R kv[K][N];   // Dopri5 FSAL: derivatives of the tangent vectors
   R h;
-  float lfac_old;  // log2 of the previous accepted step's error (>= log2 1e-4)
+  typename CtlReal<R>::type lfac_old;  // log2 of the previous accepted step's error (>= log2 1e-4)
   int32_t phase;
   bool reject;
   double t_phase, phase_len;  // time into the current phase, its length
@@ -441,11 +517,14 @@ struct PairTangentStages {  // two tangent vectors at the recorded stage points
 // Attempt one step of length h; the tangent vectors only when `joint`.
 // Returns the mean square of the weighted error components (err^2).
 template <class M, int K, class R, int INTEG>
-CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol, float atol,
-                    R (&x1)[M::N], R (&V1)[K][M::N], R (&kx1)[M::N], R (&kv1)[K][M::N]) {
+CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint,
+                                        typename CtlReal<R>::type rtol,
+                                        typename CtlReal<R>::type atol, R (&x1)[M::N],
+                                        R (&V1)[K][M::N], R (&kx1)[M::N], R (&kv1)[K][M::N]) {
+  using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
   constexpr int S = (INTEG == kDverk65) ? 8 : 7;
-  const float inv_nc = joint ? 1.0f / (N * (1 + K)) : 1.0f / N;
+  const C inv_nc = joint ? C(1) / C(N * (1 + K)) : C(1) / C(N);
   R X[S][N];
   if constexpr (Packed<M, K, R>::value) {
     constexpr bool SP = Packed<M, K, R>::state_paired;
@@ -503,7 +582,7 @@ CL_HD float attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint, float rtol,
     }
     return err2 * inv_nc;
   } else {
-    float err2 = 0.f;
+    C err2 = C(0);
     StateStages<M, R> fs{st.p, X};
     if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
     else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
@@ -631,7 +710,7 @@ CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
 #pragma unroll
     for (int j = 0; j < N; j++) L.V[i][j] = (i == j) ? R(1) : R(0);
   refresh_tangent_derivs(L);
-  L.lfac_old = kLog2FacMin;
+  L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.t_phase = 0.0;
   L.t_gs = 0.f;
   if (a.t_align > 0) {
@@ -653,12 +732,12 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
 #pragma unroll
   for (int i = 0; i < N; i++) L.x[i] = (R)a.inits.base[pt * a.inits.ps + i * a.inits.cs];
   L.h = (R)a.h0;
-  L.lfac_old = kLog2FacMin;
+  L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.reject = false;
   L.steps = 0;
   cs.t_avg = a.t_avg_per_point ? a.t_avg_per_point[pt] : a.t_avg;
   L.L = (float)a.dt_renorm / kRenormSplitInit;
-  L.rate_max = 0.f;
+  L.rate_max = initial_renorm_rate(renorm_spread_limit<R>((float)a.rtol), (float)a.dt_renorm);
 #pragma unroll
   for (int i = 0; i < K; i++) {
     cs.sum[i] = cs.comp[i] = 0.0;
@@ -703,18 +782,11 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
     }
     if (flush) lane_flush_logs(L);
   }
-  if (L.t_gs > 0.f) {  // cancellation per unit time -> next interval
-    // The rate varies along an orbit (bursts of strong contraction), so the
-    // interval follows the largest recent rate, forgotten slowly.  These
-    // quantities only steer the interval: single precision, fast division.
-    const float rate = fast_div(0.5f * 0.6931471805599453f * fast_log2f(cancel), L.t_gs);
-    L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
-    const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
-    const float dt = (float)a.dt_renorm;
-    // Growth is limited to 2x per renormalisation: a calm stretch (the first
-    // interval of a phase, the slow part of an orbit) must not open an
-    // interval long enough to cross a contraction burst unrenormalised.
-    L.L = fminf(fminf(dt, 2.0f * L.L), fmaxf(dt * (1.0f / kRenormSplitMax), target));
+  if (L.t_gs > 0.f) {  // strain per unit time -> next interval
+    double rmin = r[0];
+#pragma unroll
+    for (int i = 1; i < K; i++) rmin = fmin(rmin, r[i]);
+    next_renorm_interval(L.L, L.rate_max, cancel, rmin, L.t_gs, c.tau, (float)a.dt_renorm);
   }
   L.t_gs = 0.f;
   refresh_tangent_derivs(L);
@@ -725,9 +797,8 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
 // kFinished once the point's outputs are written.
 template <class M, int K, class R, int INTEG>
 CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
+  using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
-  constexpr float beta = 0.04f;
-  constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
   if (L.steps >= c.max_steps) {
     lane_finish(L, a, 3);
     return kFinished;
@@ -742,21 +813,14 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
   const bool joint = L.phase != kTransient;
   R x1[N], V1[K][N], kx1[N], kv1[K][N];
   L.steps++;
-  const float err2 = attempt<M, K, R, INTEG>(L, h, joint, c.rtol, c.atol, x1, V1, kx1, kv1);
-  if (!(err2 <= 3.4e38f)) {  // NaN or an overflowed error norm
+  const C err2 = attempt<M, K, R, INTEG>(L, h, joint, ctl_rtol<R>(c), ctl_atol<R>(c), x1, V1,
+                                         kx1, kv1);
+  if (!(err2 <= err2_limit<C>())) {  // NaN or an overflowed error norm
     lane_finish(L, a, 1);
     return kFinished;
   }
-  // The controller of dopri.dp.cpp:46-138 in the log2 domain: with
-  // l = log2 err, fac = err^expo1 fac_old^-beta / safe clamped to
-  // [facc2, facc1] = [0.1, 5] becomes lf = expo1 l - beta l_old - log2 safe
-  // clamped to [log2 0.1, log2 5], and h_new = h 2^-lf.
-  const float lerr = 0.5f * fast_log2f(fmaxf(err2, 1e-38f));
-  if (err2 <= 1.0f) {
-    const float lf = fminf(kLog2Facc1, fmaxf(kLog2Facc2, fmaf(expo1, lerr, fmaf(-beta, L.lfac_old,
-                                                                                   -kLog2Safe))));
-    R hnew = h * (R)exp2f(-lf);
-    L.lfac_old = fmaxf(lerr, kLog2FacMin);
+  R hnew;
+  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {
 #pragma unroll
     for (int j = 0; j < N; j++) {
       L.x[j] = x1[j];
@@ -771,9 +835,6 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
           if (INTEG == kDopri5) L.kv[i][j] = kv1[i][j];
         }
     }
-    if ((double)hnew > c.hmax) hnew = (R)c.hmax;
-    if (L.reject && hnew > h) hnew = h;
-    L.reject = false;
     if (!clamped || hnew < h) L.h = hnew;  // else keep the unclamped proposal
     L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
     L.t_gs += (float)h;
@@ -802,8 +863,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
       }
     }
   } else {
-    L.h = h * (R)exp2f(-fminf(kLog2Facc1, fmaf(expo1, lerr, -kLog2Safe)));
-    L.reject = true;
+    L.h = hnew;
   }
   return kRunning;
 }
@@ -812,7 +872,7 @@ template <class R>
 CL_HD Ctl make_ctl(const AdaptiveArgs &a) {
   // A step below 1e-12 (model time units) is never meaningful here; it also
   // stops a point whose controller collapsed the step to zero.
-  return Ctl{(float)a.rtol, (float)a.atol, renorm_spread_limit<R>((float)a.rtol),
+  return Ctl{(float)a.rtol, (float)a.atol, renorm_spread_limit<R>((float)a.rtol), a.rtol, a.atol,
              a.hmax > 0 ? a.hmax : 1e300, fmax(a.hmin, 1e-12), a.max_steps,
              a.escape > 0 ? a.escape : 1e4};
 }

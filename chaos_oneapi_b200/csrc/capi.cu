@@ -13,6 +13,7 @@
 #include "../../include/chaos_lyap.h"
 #include "kernels.h"
 #include "models.cuh"
+#include "trajectory.cuh"
 
 namespace {
 
@@ -177,57 +178,96 @@ int chaos_lyap_model_text(const char *name, int which, char *buf, int buflen) {
                                       : fail(CHAOS_LYAP_EINVAL, "buffer too small");
 }
 
-static int check_desc(const chaos_lyap_desc *d, const ModelInfo **mout) {
-  if (!d) return fail(CHAOS_LYAP_EINVAL, "desc is null");
+}  // extern "C"
+
+namespace chaos {
+static int msg_fail(char *msg, size_t len, int code, const char *fmt, ...)
+    __attribute__((format(printf, 4, 5)));
+static int msg_fail(char *msg, size_t len, int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(msg, len, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+// Descriptor validation shared by the handle path (chaos_lyap_create) and
+// the no-allocation batch entry: CHAOS_LYAP_OK, or an error code with the
+// reason in msg.  k must already be resolved (k == 0 means "dim" only at
+// create time).
+int validate_desc(const chaos_lyap_desc *d, char *msg, size_t len) {
+  if (!d) return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "desc is null");
   if (d->struct_size != (int32_t)sizeof(chaos_lyap_desc))
-    return fail(CHAOS_LYAP_EINVAL, "desc.struct_size %d != %d", d->struct_size,
+    return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "desc.struct_size %d != %d", d->struct_size,
                 (int)sizeof(chaos_lyap_desc));
   char name[33];
   std::memcpy(name, d->model, 32);
   name[32] = 0;
   const ModelInfo *m = find_model(name);
-  if (!m) return fail(CHAOS_LYAP_ENOMODEL, "unknown model '%s'", name);
-  *mout = m;
+  if (!m) return msg_fail(msg, len, CHAOS_LYAP_ENOMODEL, "unknown model '%s'", name);
   if (d->k < 1 || d->k > m->dim)
-    return fail(CHAOS_LYAP_EINVAL, "k = %d outside 1..%d for model %s", d->k, m->dim, m->name);
+    return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+        "k = %d outside 1..%d for model %s", d->k, m->dim, m->name);
   if (d->layout != CHAOS_LAYOUT_POINT_MAJOR && d->layout != CHAOS_LAYOUT_COMP_MAJOR)
-    return fail(CHAOS_LYAP_EINVAL, "bad layout %d", d->layout);
+    return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "bad layout %d", d->layout);
   if (d->method < CHAOS_METHOD_FD || d->method > CHAOS_METHOD_QR)
-    return fail(CHAOS_LYAP_EINVAL, "bad method %d", d->method);
-  if (!(d->h > 0) || !std::isfinite(d->h)) return fail(CHAOS_LYAP_EINVAL, "h must be > 0");
+    return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "bad method %d", d->method);
+  if (!(d->h > 0) || !std::isfinite(d->h)) return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+      "h must be > 0");
   if (d->precision == CHAOS_PREC_COMPAT_FP64) {
     if (d->integrator != CHAOS_INTEG_DVERK_FIXED)
-      return fail(CHAOS_LYAP_EINVAL, "compat precision needs the fixed-step DVERK integrator");
+      return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+          "compat precision needs the fixed-step DVERK integrator");
     if (d->method == CHAOS_METHOD_QR && d->k != m->dim)
-      return fail(CHAOS_LYAP_EUNSUPPORTED,
+      return msg_fail(msg, len, CHAOS_LYAP_EUNSUPPORTED,
                   "QR method needs k == dim (the reference's QR assumes a square matrix)");
-    if (!(d->t_avg > 0)) return fail(CHAOS_LYAP_EINVAL, "t_avg must be > 0");
+    if (!(d->t_avg > 0)) return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "t_avg must be > 0");
   } else if (d->precision == CHAOS_PREC_FP64 || d->precision == CHAOS_PREC_FP32) {
     if (d->integrator != CHAOS_INTEG_DVERK65 && d->integrator != CHAOS_INTEG_DOPRI5)
-      return fail(CHAOS_LYAP_EINVAL, "adaptive precision forms need DVERK65 or DOPRI5");
+      return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+          "adaptive precision forms need DVERK65 or DOPRI5");
     if (d->method != CHAOS_METHOD_VAR)
-      return fail(CHAOS_LYAP_EUNSUPPORTED, "adaptive forms integrate the variational equations (VAR)");
+      return msg_fail(msg, len, CHAOS_LYAP_EUNSUPPORTED,
+          "adaptive forms integrate the variational equations (VAR)");
     if (d->k != m->dim && m->dim <= 4)
-      return fail(CHAOS_LYAP_EUNSUPPORTED, "adaptive forms compute the full spectrum (k == dim)");
-    if (!(d->rtol > 0) || !(d->atol > 0)) return fail(CHAOS_LYAP_EINVAL, "rtol/atol must be > 0");
+      return msg_fail(msg, len, CHAOS_LYAP_EUNSUPPORTED,
+          "adaptive forms compute the full spectrum (k == dim)");
+    if (!(d->rtol > 0) || !(d->atol > 0)) return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+        "rtol/atol must be > 0");
     if (!(d->dt_renorm > 0) || !(d->t_avg > 0) || d->t_transient < 0 || d->t_align < 0)
-      return fail(CHAOS_LYAP_EINVAL, "times: dt_renorm, t_avg > 0; t_transient, t_align >= 0");
-    if (d->max_steps <= 0) return fail(CHAOS_LYAP_EINVAL, "max_steps must be > 0");
+      return msg_fail(msg, len, CHAOS_LYAP_EINVAL,
+          "times: dt_renorm, t_avg > 0; t_transient, t_align >= 0");
+    if (d->max_steps <= 0) return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "max_steps must be > 0");
     if (d->gs != CHAOS_GS_CLASSICAL && d->gs != CHAOS_GS_MODIFIED)
-      return fail(CHAOS_LYAP_EINVAL, "bad gs %d", d->gs);
+      return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "bad gs %d", d->gs);
   } else {
-    return fail(CHAOS_LYAP_EINVAL, "bad precision %d", d->precision);
+    return msg_fail(msg, len, CHAOS_LYAP_EINVAL, "bad precision %d", d->precision);
   }
   if (m->type != 0) {  // maps: the reference's FD / VAR map branches, in compat precision
     if (d->precision != CHAOS_PREC_COMPAT_FP64)
-      return fail(CHAOS_LYAP_EUNSUPPORTED,
+      return msg_fail(msg, len, CHAOS_LYAP_EUNSUPPORTED,
                   "map model %s: maps are iterated, not integrated; use compat precision", m->name);
     if (d->method == CHAOS_METHOD_QR)
-      return fail(CHAOS_LYAP_EUNSUPPORTED, "map model %s: the QR method has no map branch",
+      return msg_fail(msg, len, CHAOS_LYAP_EUNSUPPORTED,
+          "map model %s: the QR method has no map branch",
                   m->name);
   }
   return CHAOS_LYAP_OK;
 }
+}  // namespace chaos
+
+static int check_desc(const chaos_lyap_desc *d, const ModelInfo **mout) {
+  char msg[512];
+  const int rc = chaos::validate_desc(d, msg, sizeof msg);
+  if (rc) return fail(rc, "%s", msg);
+  char name[33];
+  std::memcpy(name, d->model, 32);
+  name[32] = 0;
+  *mout = find_model(name);
+  return CHAOS_LYAP_OK;
+}
+
+extern "C" {
 
 int chaos_lyap_create(const chaos_lyap_desc *desc, chaos_lyap_handle **out) {
   if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
@@ -544,20 +584,46 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
 struct BatchPlan {
   chaos::BatchArgs lane, split;
   chaos_lyap_handle *lane_h[chaos::kMaxSegments], *split_h[chaos::kMaxSegments];
+  // scratch of the longest-first ordering of each segment with per-point times
+  void *lane_scratch[chaos::kMaxSegments], *split_scratch[chaos::kMaxSegments];
   int integ, prec, lane_block, split_block;
+};
+
+// Device buffers of one segment's longest-first hand-out order.
+struct OrderBuf {
+  int32_t *order;
+  void *scratch;
 };
 
 static bool is_split(const chaos_lyap_handle *h) {
   return h->schedule == CHAOS_SCHED_SPLIT_DIRECT || h->schedule == CHAOS_SCHED_SPLIT_PERSISTENT;
 }
 
-static int build_batch(const chaos_lyap_segment *segs, int nseg, BatchPlan *plan) {
+// Checks the segments and lays out the launch.  Each segment's longest-first
+// order goes into `own[i]` when given (buffers a graph owns, sized for the
+// segment), else into the segment handle's own buffers (grown on demand).
+// Every segment has its own handle: two segments of one handle would share
+// that handle's order buffer.
+static int check_segments(const chaos_lyap_segment *segs, int nseg) {
   if (!segs || nseg <= 0 || nseg > chaos::kMaxSegments)
     return fail(CHAOS_LYAP_EINVAL, "nseg must be 1..%d", chaos::kMaxSegments);
+  for (int i = 0; i < nseg; i++) {
+    if (!segs[i].handle) return fail(CHAOS_LYAP_EINVAL, "segment %d: null handle", i);
+    for (int j = 0; j < i; j++)
+      if (segs[j].handle == segs[i].handle)
+        return fail(CHAOS_LYAP_EINVAL,
+                    "segments %d and %d share a handle: every segment needs its own", j, i);
+  }
+  return CHAOS_LYAP_OK;
+}
+
+static int build_batch(const chaos_lyap_segment *segs, int nseg, BatchPlan *plan,
+                       const OrderBuf *own) {
+  int rc0 = check_segments(segs, nseg);
+  if (rc0) return rc0;
   std::memset(plan, 0, sizeof *plan);
   for (int i = 0; i < nseg; i++) {
     const chaos_lyap_segment &sg = segs[i];
-    if (!sg.handle) return fail(CHAOS_LYAP_EINVAL, "segment %d: null handle", i);
     const chaos_lyap_desc &d = sg.handle->d;
     if (d.precision == CHAOS_PREC_COMPAT_FP64 || sg.handle->model->dim > 4)
       return fail(CHAOS_LYAP_EUNSUPPORTED,
@@ -596,11 +662,19 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, BatchPlan *plan
     a.steps = sg.steps;
     a.queue_stride = chaos::queue_stride_for(sg.P);
     a.order = nullptr;
+    void *scratch = nullptr;
     if (sg.t_avg_per_point && sg.P > 0) {  // longest averaging time first
-      int rc = ensure_order(sg.handle, sg.P);
-      if (rc) return rc;
-      a.order = sg.handle->order;
+      if (own) {
+        a.order = own[i].order;
+        scratch = own[i].scratch;
+      } else {
+        int rc = ensure_order(sg.handle, sg.P);
+        if (rc) return rc;
+        a.order = sg.handle->order;
+        scratch = sg.handle->order_scratch;
+      }
     }
+    (sp ? plan->split_scratch : plan->lane_scratch)[j] = scratch;
     b.model[j] = m->id;
   }
   chaos_lyap_handle *h0 = segs[0].handle;
@@ -622,11 +696,11 @@ static int build_batch(const chaos_lyap_segment *segs, int nseg, BatchPlan *plan
   return CHAOS_LYAP_OK;
 }
 
-static int launch_orders(const chaos::BatchArgs &b, chaos_lyap_handle *const *hs, cudaStream_t s) {
+static int launch_orders(const chaos::BatchArgs &b, void *const *scratch, cudaStream_t s) {
   for (int i = 0; i < b.nseg; i++) {
     if (!b.seg[i].order) continue;
-    int rc = chaos::launch_order_longest_first(b.seg[i].t_avg_per_point, b.seg[i].P, hs[i]->order,
-                                               hs[i]->order_scratch, s);
+    int rc = chaos::launch_order_longest_first(b.seg[i].t_avg_per_point, b.seg[i].P,
+                                               const_cast<int32_t *>(b.seg[i].order), scratch[i], s);
     if (rc) return cuda_fail((cudaError_t)rc, "order launch");
   }
   return CHAOS_LYAP_OK;
@@ -642,8 +716,8 @@ static int enqueue_batch(const BatchPlan &p, chaos_lyap_handle *h0, cudaStream_t
   const int nseg = p.lane.nseg + p.split.nseg;
   cudaError_t e = cudaMemsetAsync(h0->queue, 0, sizeof(unsigned long long) * nseg, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(queues)");
-  int rc = launch_orders(p.lane, p.lane_h, s);
-  if (!rc) rc = launch_orders(p.split, p.split_h, s);
+  int rc = launch_orders(p.lane, p.lane_scratch, s);
+  if (!rc) rc = launch_orders(p.split, p.split_scratch, s);
   if (rc) return rc;
   if (p.lane.nseg && p.split.nseg) {
     cudaStream_t aux = h0->aux_stream;
@@ -665,7 +739,7 @@ static int enqueue_batch(const BatchPlan &p, chaos_lyap_handle *h0, cudaStream_t
 
 int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream) {
   BatchPlan plan;
-  int rc = build_batch(segs, nseg, &plan);
+  int rc = build_batch(segs, nseg, &plan, nullptr);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
   rc = enqueue_batch(plan, segs[0].handle, (cudaStream_t)stream);
@@ -673,24 +747,55 @@ int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream)
   return rc;
 }
 
+// A captured batch.  The graph owns the longest-first order buffers of its
+// segments, so a later run on one of its handles (which may regrow that
+// handle's own buffer) cannot leave the graph reading freed memory.
 struct chaos_lyap_graph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
+  OrderBuf order[chaos::kMaxSegments] = {};
 };
+
+static void free_graph(chaos_lyap_graph *gr) {
+  if (gr->exec) cudaGraphExecDestroy(gr->exec);
+  if (gr->graph) cudaGraphDestroy(gr->graph);
+  for (auto &o : gr->order) {
+    cudaFree(o.order);
+    cudaFree(o.scratch);
+  }
+  delete gr;
+}
 
 int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chaos_lyap_graph **out) {
   if (!out) return fail(CHAOS_LYAP_EINVAL, "out is null");
   *out = nullptr;
-  BatchPlan plan;
-  int rc = build_batch(segs, nseg, &plan);
+  int rc = check_segments(segs, nseg);
   if (rc) return rc;
   DeviceGuard g(segs[0].handle->d.device);
-  cudaStream_t cs;
-  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
   auto *gr = new chaos_lyap_graph();
   gr->device = segs[0].handle->d.device;
+  for (int i = 0; i < nseg; i++) {
+    if (!segs[i].t_avg_per_point || segs[i].P <= 0) continue;
+    cudaError_t e = cudaMalloc(&gr->order[i].order, sizeof(int32_t) * segs[i].P);
+    if (e == cudaSuccess) e = cudaMalloc(&gr->order[i].scratch, chaos::kOrderScratchBytes);
+    if (e != cudaSuccess) {
+      free_graph(gr);
+      return fail(CHAOS_LYAP_ENOMEM, "cudaMalloc(graph order): %s", cudaGetErrorString(e));
+    }
+  }
+  BatchPlan plan;
+  rc = build_batch(segs, nseg, &plan, gr->order);
+  if (rc) {
+    free_graph(gr);
+    return rc;
+  }
+  cudaStream_t cs;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    free_graph(gr);
+    return cuda_fail(e, "cudaStreamCreate");
+  }
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     rc = enqueue_batch(plan, segs[0].handle, cs);
@@ -705,9 +810,7 @@ int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chao
     rc = cuda_fail(e, "cudaGraphInstantiate");
   cudaStreamDestroy(cs);
   if (rc) {
-    if (gr->exec) cudaGraphExecDestroy(gr->exec);
-    if (gr->graph) cudaGraphDestroy(gr->graph);
-    delete gr;
+    free_graph(gr);
     return rc;
   }
   *out = gr;
@@ -724,9 +827,51 @@ int chaos_lyap_graph_launch(chaos_lyap_graph *g, void *stream) {
 int chaos_lyap_graph_destroy(chaos_lyap_graph *g) {
   if (!g) return CHAOS_LYAP_OK;
   DeviceGuard dg(g->device);
-  cudaGraphExecDestroy(g->exec);
-  cudaGraphDestroy(g->graph);
-  delete g;
+  free_graph(g);
+  return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_trajectory(chaos_lyap_handle *h, int64_t P, const double *params,
+                          const double *inits, int32_t nsteps, double *t_out, double *h_out,
+                          double *x_out, int32_t *status, void *stream) {
+  if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
+  const chaos_lyap_desc &d = h->d;
+  const ModelInfo *m = h->model;
+  if (d.precision == CHAOS_PREC_COMPAT_FP64)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "trajectories take the adaptive forms (FP64 or FP32)");
+  if (m->type != 0 || m->dim > 4)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "trajectories of flows of dimension <= 4 (model %s)",
+                m->name);
+  if (P < 0 || nsteps < 0) return fail(CHAOS_LYAP_EINVAL, "P and nsteps must be >= 0");
+  if (P == 0 || nsteps == 0) return CHAOS_LYAP_OK;
+  if (!params || !inits || !t_out || !h_out || !x_out) return fail(CHAOS_LYAP_EINVAL, "null array");
+  DeviceGuard g(d.device);
+  if (!g.ok) return fail(CHAOS_LYAP_ECUDA, "cannot select device %d", d.device);
+  chaos::adaptive::TrajectoryArgs ta{};
+  chaos::AdaptiveArgs &a = ta.a;
+  a.P = P;
+  a.k = m->dim;
+  a.rtol = d.rtol;
+  a.atol = d.atol;
+  a.h0 = d.h;
+  a.hmax = d.h_max;
+  a.hmin = d.h_min;
+  a.max_steps = d.max_steps;
+  a.escape = d.escape > 0 ? d.escape : 1e4;
+  a.params = cview(params, P, m->nparams, d.layout);
+  a.inits = cview(inits, P, m->dim, d.layout);
+  ta.nsteps = nsteps;
+  ta.t_out = t_out;
+  ta.h_out = h_out;
+  ta.x_out = x_out;
+  ta.status = status;
+  const int integ = d.integrator == CHAOS_INTEG_DOPRI5 ? chaos::kDopri5 : chaos::kDverk65;
+  const int prec = d.precision == CHAOS_PREC_FP32 ? chaos::kFP32 : chaos::kFP64;
+  const int rc = chaos::launch_trajectory(m->id, integ, prec, ta, (cudaStream_t)stream);
+  if (rc == chaos::kErrUnsupported)
+    return fail(CHAOS_LYAP_EUNSUPPORTED, "no trajectory kernel for model %s", m->name);
+  if (rc) return cuda_fail((cudaError_t)rc, "trajectory launch");
+  h->last_stream = (cudaStream_t)stream;
   return CHAOS_LYAP_OK;
 }
 

@@ -16,14 +16,16 @@
 // 4 x k x 40 floats per warp; the FP64 QR reuses the candidate half.
 //
 // The phase and renormalisation logic follows adaptive.cuh (transient /
-// alignment / averaging with clamped landings, interval from the
-// Gram-Schmidt cancellation factor, norm products flushed into Kahan sums,
-// escape radius, step budget); every decision is warp-uniform.
+// alignment / averaging with clamped landings, the renormalisation interval
+// of renorm.cuh from the Gram-Schmidt cancellation and the shrinking of the
+// norms, norm products flushed into Kahan sums, escape radius, step budget);
+// every decision is warp-uniform.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "kernels.h"
+#include "renorm.cuh"
 
 namespace chaos {
 namespace l96 {
@@ -213,12 +215,13 @@ __device__ void refresh_kv(const Warp &w, const float *V, float *KV, int k, int 
 // the FP64 work area W (k x 40 doubles).  Returns max |v_q|^2 / r_q^2 (the
 // cancellation factor) and multiplies r_q into the lane that owns exponent q.
 __device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int lane,
-                         bool accumulate, bool &ok) {
+                         bool accumulate, bool &ok, double &rmin) {
   // FP32 -> FP64, and squared norms before orthogonalisation
   for (int idx = lane; idx < k * N; idx += 32) W[idx] = (double)V[idx];
   __syncwarp();
   double cancel = 1.0;
   ok = true;
+  rmin = 1e300;
   for (int q = 0; q < k; q++) {
     double wq[C];
 #pragma unroll
@@ -230,6 +233,7 @@ __device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int
     const double inv = rsqrt(s);
     const double r = s * inv;
     ok = ok && (r > 0.0) && (r < 1e300);
+    rmin = fmin(rmin, r);
 #pragma unroll
     for (int j = 0; j < C; j++) wq[j] *= inv;
     __syncwarp();
@@ -349,8 +353,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
     w.reject = false;
     w.steps = 0;
     w.t_avg = a.t_avg_per_point ? a.t_avg_per_point[w.pt] : a.t_avg;
-    w.L = a.dt_renorm / 16;
-    w.rate_max = 0.0;
+    w.L = a.dt_renorm / adaptive::kRenormSplitInit;
+    w.rate_max = adaptive::initial_renorm_rate(tau, (float)a.dt_renorm);
 #pragma unroll
     for (int i = 0; i < 2; i++) w.sum[i] = w.comp[i] = 0.0, w.prod[i] = 1.0;
     Jc jc;
@@ -367,7 +371,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
   // Gram-Schmidt of the warp's point; false on a degenerate basis.
   auto gram_schmidt = [&]() -> bool {
     bool ok;
-    const double cancel = mgs_qr(w, V, W, k, g, li, lane, w.phase == kAverage, ok);
+    double rmin;
+    const double cancel = mgs_qr(w, V, W, k, g, li, lane, w.phase == kAverage, ok, rmin);
     if (!ok) return false;
     if (w.phase == kAverage) {
       bool fl = false;
@@ -375,12 +380,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
       for (int i = 0; i < 2; i++) fl = fl || !(w.prod[i] < 1e150 && w.prod[i] > 1e-150);
       if (__any_sync(FULL, fl)) flush_logs(w);
     }
-    if (w.t_gs > 0.0) {
-      const double rate = 0.5 * (double)logf((float)cancel) / w.t_gs;
-      w.rate_max = fmax(rate, 0.995 * w.rate_max);
-      const double target = 0.125 * tau / fmax(w.rate_max, 1e-30);
-      w.L = fmin(fmin(a.dt_renorm, 2.0 * w.L), fmax(a.dt_renorm / 64, target));  // grows <= 2x
-    }
+    if (w.t_gs > 0.0)  // the policy of every adaptive form (renorm.cuh)
+      adaptive::next_renorm_interval(w.L, w.rate_max, (float)cancel, rmin, w.t_gs, tau,
+                                     a.dt_renorm);
     w.t_gs = 0.0;
     refresh_kv(w, V, KV, k, g, li, left, right);
     return true;

@@ -41,7 +41,7 @@ __device__ __forceinline__ Group group_of() {
   return Group{lane & 3, lane & ~3, 0xFu << (lane & ~3)};
 }
 
-__device__ __forceinline__ float group_sum(float e, unsigned mask) {
+template <class T> __device__ __forceinline__ T group_sum(T e, unsigned mask) {
   e += __shfl_xor_sync(mask, e, 1);
   e += __shfl_xor_sync(mask, e, 2);
   return e;
@@ -60,7 +60,7 @@ struct SplitLane {
   R v[N];         // this lane's tangent vector (zero for rows >= k)
   R kx[N], kv[N]; // Dopri5 FSAL derivatives
   R h;
-  float lfac_old;
+  typename CtlReal<R>::type lfac_old;
   int32_t phase;
   bool reject;
   double t_phase, phase_len;
@@ -101,7 +101,7 @@ __device__ void split_start_tangent(SplitLane<M, R, INTEG> &L, const AdaptiveArg
 #pragma unroll
   for (int j = 0; j < N; j++) L.v[j] = (j == g.r) ? R(1) : R(0);
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
-  L.lfac_old = kLog2FacMin;
+  L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.t_phase = 0.0;
   L.t_gs = 0.f;
   if (a.t_align > 0) {
@@ -128,11 +128,11 @@ __device__ void split_start(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, in
 #pragma unroll
   for (int j = 0; j < N; j++) L.v[j] = L.kv[j] = R(0);
   L.h = (R)a.h0;
-  L.lfac_old = kLog2FacMin;
+  L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.reject = false;
   L.steps = 0;
   L.L = (float)a.dt_renorm / kRenormSplitInit;
-  L.rate_max = 0.f;
+  L.rate_max = initial_renorm_rate(renorm_spread_limit<R>((float)a.rtol), (float)a.dt_renorm);
   L.prod = 1.0;
   if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
   if (a.t_transient > 0) {
@@ -148,12 +148,16 @@ __device__ void split_start(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, in
 // One step attempt: the state and this lane's vector; returns the group's
 // mean square weighted error (the same in all four lanes).
 template <class M, class R, int INTEG>
-__device__ float split_attempt(const SplitLane<M, R, INTEG> &st, R h, bool joint, bool has_vec,
-                               const Group &g, float rtol, float atol, R (&x1)[M::N],
-                               R (&v1)[M::N], R (&kx1)[M::N], R (&kv1)[M::N]) {
+__device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG> &st, R h,
+                                                   bool joint, bool has_vec, const Group &g,
+                                                   typename CtlReal<R>::type rtol,
+                                                   typename CtlReal<R>::type atol,
+                                                   R (&x1)[M::N], R (&v1)[M::N],
+                                                   R (&kx1)[M::N], R (&kv1)[M::N]) {
+  using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
   constexpr int S = (INTEG == kDverk65) ? 8 : 7;
-  float es = 0.f, ev = 0.f;
+  C es = C(0), ev = C(0);
   if constexpr (std::is_same<R, float>::value) {  // (state, v_r) as one packed pass
     float X[S][N];
     float2 ya[N], ka[N], ya1[N], ka1[N];
@@ -189,9 +193,9 @@ __device__ float split_attempt(const SplitLane<M, R, INTEG> &st, R h, bool joint
     }
   }
   // the state's error once (lane 0), each vector's in its own lane
-  float e = (g.r == 0 ? es : 0.f) + ((joint && has_vec) ? ev : 0.f);
+  C e = (g.r == 0 ? es : C(0)) + ((joint && has_vec) ? ev : C(0));
   e = group_sum(e, g.mask);
-  const float inv_nc = joint ? 1.0f / (N * (1 + M::N)) : 1.0f / N;
+  const C inv_nc = joint ? C(1) / C(N * (1 + M::N)) : C(1) / C(N);
   return e * inv_nc;
 }
 
@@ -247,17 +251,15 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
 #pragma unroll
   for (int j = 0; j < N; j++) L.v[j] = has_vec ? (R)w[j] : R(0);
   cancel = group_max(cancel, g.mask);
+  double rmin = has_vec ? rr : 1.0;
+  rmin = fmin(rmin, __shfl_xor_sync(g.mask, rmin, 1));
+  rmin = fmin(rmin, __shfl_xor_sync(g.mask, rmin, 2));
   if (L.phase == kAverage && has_vec) {
     L.prod *= rr;
     if (!(L.prod < 1e150 && L.prod > 1e-150)) split_flush(L);
   }
-  if (L.t_gs > 0.f) {  // the interval rule of the one-lane form, on the group's max
-    const float rate = fast_div(0.5f * 0.6931471805599453f * fast_log2f(cancel), L.t_gs);
-    L.rate_max = fmaxf(rate, 0.995f * L.rate_max);
-    const float target = fast_div(0.125f * c.tau, fmaxf(L.rate_max, 1e-30f));
-    const float dt = (float)a.dt_renorm;
-    L.L = fminf(fminf(dt, 2.0f * L.L), fmaxf(dt * (1.0f / kRenormSplitMax), target));
-  }
+  if (L.t_gs > 0.f)  // the interval rule of the one-lane form, on the group's extremes
+    next_renorm_interval(L.L, L.rate_max, cancel, rmin, L.t_gs, c.tau, (float)a.dt_renorm);
   L.t_gs = 0.f;
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
   return true;
@@ -268,9 +270,8 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
 template <class M, class R, int INTEG>
 __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c,
                           const Group &g) {
+  using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
-  constexpr float beta = 0.04f;
-  constexpr float expo1 = (INTEG == kDverk65 ? 1.0f / 6.0f : 0.2f) - beta * 0.75f;
   if (L.steps >= c.max_steps) {
     split_finish(L, a, g, 3);
     return kFinished;
@@ -286,18 +287,14 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
   const bool has_vec = g.r < M::N;  // launches take k == dim
   R x1[N], v1[N], kx1[N], kv1[N];
   L.steps++;
-  const float err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, c.rtol, c.atol, x1, v1,
-                                                kx1, kv1);
-  if (!(err2 <= 3.4e38f)) {
+  const C err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, ctl_rtol<R>(c),
+                                            ctl_atol<R>(c), x1, v1, kx1, kv1);
+  if (!(err2 <= err2_limit<C>())) {
     split_finish(L, a, g, 1);
     return kFinished;
   }
-  const float lerr = 0.5f * fast_log2f(fmaxf(err2, 1e-38f));
-  if (err2 <= 1.0f) {
-    const float lf = fminf(kLog2Facc1, fmaxf(kLog2Facc2, fmaf(expo1, lerr, fmaf(-beta, L.lfac_old,
-                                                                                   -kLog2Safe))));
-    R hnew = h * (R)exp2f(-lf);
-    L.lfac_old = fmaxf(lerr, kLog2FacMin);
+  R hnew;
+  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {
 #pragma unroll
     for (int j = 0; j < N; j++) {
       L.x[j] = x1[j];
@@ -310,9 +307,6 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
         if (INTEG == kDopri5) L.kv[j] = kv1[j];
       }
     }
-    if ((double)hnew > c.hmax) hnew = (R)c.hmax;
-    if (L.reject && hnew > h) hnew = h;
-    L.reject = false;
     if (!clamped || hnew < h) L.h = hnew;
     L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
     L.t_gs += (float)h;
@@ -341,8 +335,7 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
       }
     }
   } else {
-    L.h = h * (R)exp2f(-fminf(kLog2Facc1, fmaf(expo1, lerr, -kLog2Safe)));
-    L.reject = true;
+    L.h = hnew;
   }
   return kRunning;
 }

@@ -23,7 +23,10 @@
 //   * the counters keep the previous call's values; each call zeroes the ones
 //     it uses (cudaMemsetAsync on the caller's stream) before its launch;
 //   * the first call on a device performs the address lookup above; make that
-//     first call before any stream capture begins.
+//     first call before any stream capture begins;
+//   * the address is remembered for the life of the process: the entry point
+//     does not survive a reset of the device (cudaDeviceReset, or anything
+//     else that destroys and recreates its primary context).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -32,6 +35,11 @@
 
 #include "../../include/chaos_lyap.h"
 #include "kernels.h"
+
+namespace chaos {
+// Descriptor validation shared with the handle path (capi.cu).
+int validate_desc(const chaos_lyap_desc *d, char *msg, size_t len);
+}  // namespace chaos
 
 namespace {
 
@@ -86,31 +94,26 @@ extern "C" int chaos_lyap_run_batch_static(const chaos_lyap_desc *descs,
   b.nseg = nseg;
   const chaos_lyap_desc &d0 = descs[0];
   for (int i = 0; i < nseg; i++) {
-    const chaos_lyap_desc &d = descs[i];
-    if (d.struct_size != (int32_t)sizeof(chaos_lyap_desc))
+    if (descs[i].struct_size != (int32_t)sizeof(chaos_lyap_desc))
       return failmsg(CHAOS_LYAP_EINVAL, "descriptor struct_size mismatch");
+    chaos_lyap_desc d = descs[i];
     char name[33];
     std::memcpy(name, d.model, 32);
     name[32] = 0;
     int dim = 0, np = 0;
     const int id = chaos::model_id_of(name, &dim, &np);
     if (id < 0) return failmsg(CHAOS_LYAP_ENOMODEL, "unknown model in a segment descriptor");
-    const int k = d.k == 0 ? dim : d.k;
-    if (dim > 4 || k != dim)
+    if (d.k == 0) d.k = dim;
+    // the handle path's checks first (maps, tolerances, times, h, layout ...)
+    const int vrc = chaos::validate_desc(&d, g_msg, sizeof g_msg);
+    if (vrc) return vrc;
+    const int k = d.k;
+    if (d.precision == CHAOS_PREC_COMPAT_FP64)
+      return failmsg(CHAOS_LYAP_EUNSUPPORTED, "segments take the adaptive forms (FP64 or FP32)");
+    if (dim < 3 || dim > 4 || k != dim)
       return failmsg(CHAOS_LYAP_EUNSUPPORTED, "segments take 3-4 dimensional models, k == dim");
-    if ((d.precision != CHAOS_PREC_FP32 && d.precision != CHAOS_PREC_FP64) ||
-        (d.integrator != CHAOS_INTEG_DOPRI5 && d.integrator != CHAOS_INTEG_DVERK65) ||
-        d.method != CHAOS_METHOD_VAR)
-      return failmsg(CHAOS_LYAP_EUNSUPPORTED, "segments take the adaptive forms (VAR method)");
     if (d.precision != d0.precision || d.integrator != d0.integrator || d.device != d0.device)
       return failmsg(CHAOS_LYAP_EINVAL, "segments differ in integrator, precision or device");
-    if (!(d.rtol > 0) || !(d.atol > 0) || !(d.dt_renorm > 0) || !(d.t_avg > 0) ||
-        d.t_transient < 0 || d.t_align < 0 || d.max_steps <= 0 || !(d.h > 0))
-      return failmsg(CHAOS_LYAP_EINVAL, "bad tolerances, times, initial step or step budget");
-    if (d.layout != CHAOS_LAYOUT_POINT_MAJOR && d.layout != CHAOS_LAYOUT_COMP_MAJOR)
-      return failmsg(CHAOS_LYAP_EINVAL, "bad layout");
-    if (d.gs != CHAOS_GS_CLASSICAL && d.gs != CHAOS_GS_MODIFIED)
-      return failmsg(CHAOS_LYAP_EINVAL, "bad Gram-Schmidt variant");
     const chaos_lyap_segment &sg = segs[i];
     if (sg.P < 0 || (sg.P > 0 && (!sg.params || !sg.inits || !sg.spectrum)))
       return failmsg(CHAOS_LYAP_EINVAL, "bad segment arrays");

@@ -94,6 +94,8 @@ SIGNATURES = {
     "chaos_lyap_graph_launch": (ctypes.c_int, [_P, _P]),
     "chaos_lyap_graph_destroy": (ctypes.c_int, [_P]),
     "chaos_lyap_get_variant": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int32)]),
+    "chaos_lyap_trajectory": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P, ctypes.c_int32, _P, _P,
+                                             _P, _P, _P]),
     "chaos_lyap_cudaLyapunov": (ctypes.c_int, [
         ctypes.c_int, ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.c_int,
         _P, _P, ctypes.c_int32, ctypes.c_char_p, _P, ctypes.c_int32, ctypes.c_double,

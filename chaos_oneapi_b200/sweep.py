@@ -208,6 +208,30 @@ class Sweep:
         return {"block": b.value, "schedule": {1: "direct", 2: "persistent", 3: "split", 4: "split_persistent"}.get(s.value, "auto"),
                 "variant": self.variant_in_use()}
 
+    def trajectory(self, params, inits, nsteps: int, stream=None):
+        """The state alone, `nsteps` accepted steps per point from time 0, the
+        way the reference's dopriStep tool is called (chaos_lyap_trajectory).
+        CUDA tensors in; returns CUDA tensors (times, step proposals, states,
+        statuses) of shapes (P, nsteps), (P, nsteps), (P, nsteps, dim), (P,),
+        enqueued on `stream` (torch's current stream when None)."""
+        import torch
+        P = params.shape[0] if self.cfg.layout == "point" else params.shape[-1]
+        dev = params.device
+        t = torch.empty((P, nsteps), dtype=torch.float64, device=dev)
+        h = torch.empty((P, nsteps), dtype=torch.float64, device=dev)
+        x = torch.empty((P, nsteps, self.dim), dtype=torch.float64, device=dev)
+        st = torch.empty(P, dtype=torch.int32, device=dev)
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        check(lib.chaos_lyap_trajectory(self._h, P, _tptr(params, "float64", P * self.nparams),
+                                        _tptr(inits, "float64", P * self.dim), nsteps,
+                                        _tptr(t, "float64"), _tptr(h, "float64"),
+                                        _tptr(x, "float64"), _tptr(st, "int32"),
+                                        ctypes.c_void_p(stream)))
+        return t, h, x, st
+
     def variant_in_use(self) -> int:
         v = ctypes.c_int32()
         check(lib.chaos_lyap_get_variant(self._h, ctypes.byref(v)))

@@ -187,8 +187,10 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
  * its own handle, arrays and phase times; per-point averaging times allowed)
  * in ONE persistent launch whose lanes take points segment after segment, so
  * points of uneven dimension and length share warps without idling them.
- * All handles must use the same integrator and precision; nseg <= 8.  The
- * point counters live in the first segment's handle.  No reference
+ * All handles must use the same integrator and precision; nseg <= 8; every
+ * segment has its own handle (a handle in two segments is rejected).  The
+ * point counters live in the first segment's handle: do not run that handle
+ * on another stream while a batch on it is in flight.  No reference
  * counterpart (the reference launches one model per run, tasklyapunov.cpp:204). */
 typedef struct chaos_lyap_segment {
   chaos_lyap_handle *handle;
@@ -205,7 +207,9 @@ int chaos_lyap_run_batch(const chaos_lyap_segment *segs, int nseg, void *stream)
 
 /* The same batch captured once into a CUDA graph (counter reset + launch)
  * and replayed by chaos_lyap_graph_launch on any stream; the segments'
- * arrays are baked in: refill them and replay. */
+ * arrays are baked in: refill them and replay.  The graph owns the buffers
+ * of its longest-first orderings, so later runs of its handles do not
+ * disturb it. */
 typedef struct chaos_lyap_graph chaos_lyap_graph;
 int chaos_lyap_batch_graph_create(const chaos_lyap_segment *segs, int nseg, chaos_lyap_graph **out);
 int chaos_lyap_graph_launch(chaos_lyap_graph *g, void *stream);
@@ -222,11 +226,35 @@ int chaos_lyap_graph_destroy(chaos_lyap_graph *g);
  * rejected.  All calls share those counters: calls that overlap on the GPU
  * race, so serialise them.  Each call zeroes the counters it uses on `stream`
  * before launching.  The first call on a device looks up the array's device
- * address; make it before any stream capture begins.  On failure the message
- * is in chaos_lyap_static_last_error(). */
+ * address; make it before any stream capture begins.  That address is kept
+ * for the life of the process: the entry point does not survive a device
+ * reset (cudaDeviceReset).  Descriptors are checked as chaos_lyap_create
+ * checks them.  On failure the message is in chaos_lyap_static_last_error(). */
 int chaos_lyap_run_batch_static(const chaos_lyap_desc *descs, const chaos_lyap_segment *segs,
                                 int nseg, void *stream);
 const char *chaos_lyap_static_last_error(void);
+
+/* State trajectories through the adaptive integrators: the reference's
+ * Dormand-Prince tool dopriStep (cuda/tools/dopri.dp.cpp:7-139, declared in
+ * cuda/tools/dopri.dp.hpp:7-8) as a batched call, one lane per point.  A
+ * caller of dopriStep starts at time 0 and makes one accepted step per call
+ * (rejections retried inside), keeping the step proposal and the FSAL
+ * derivative between calls; here every point makes `nsteps` such steps of
+ * the STATE alone with the handle's integrator (DOPRI5 as the reference,
+ * or DVERK65), precision (FP64: error norm and controller in FP64, the
+ * reference's arithmetic to rounding; FP32), rtol / atol (the reference's
+ * tolGlobErr / tolLocErr), h (initial step), h_max (maxStep; 0 = unbounded),
+ * h_min, max_steps (attempted steps) and escape radius.  DEVICE pointers:
+ *   params  P x nparams, inits P x dim (layout per desc)
+ *   t_out   P x nsteps time after each accepted step
+ *   h_out   P x nsteps the step proposal after it
+ *   x_out   P x nsteps x dim the state after it (point-major)
+ *   status  optional P int32 (CHAOS_POINT_*); records a point did not reach
+ *           are NaN.
+ * Flows of dimension <= 4.  Stream-ordered; returns after enqueueing. */
+int chaos_lyap_trajectory(chaos_lyap_handle *h, int64_t P, const double *params,
+                          const double *inits, int32_t nsteps, double *t_out, double *h_out,
+                          double *x_out, int32_t *status, void *stream);
 
 /* The FP32 kernel variant in use (desc.variant, or the autotuner's choice). */
 int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);

@@ -21,7 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(HERE, "liblyap_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libchaos_ref.so")
 REF_MAIN = os.path.join(HERE, "_ref", "chaos_ref_main")
-REF_TREE = "/root/reference"
+# where the reference's sources lie (only the build reads them)
+REF_TREE = os.environ.get("CHAOS_REF_TREE", "/root/reference")
 
 MODELS = {"shimizu": 0, "lorenz": 1, "rossler": 2, "chua": 3, "hyper_rossler": 4, "lorenz96": 5,
           "henon": 6}
@@ -69,6 +70,9 @@ def orc() -> ctypes.CDLL:
         lib.orc_make_inits.argtypes = [ctypes.c_int, ctypes.c_int64, _D, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_uint64, _D]
         lib.orc_dverk_step.argtypes = [ctypes.c_int, _D, _D, ctypes.c_double]
+        lib.orc_dopri_trajectory.argtypes = [ctypes.c_int, _D, _D, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_int, _D, _D, _D]
         _orc = lib
     return _orc
 
@@ -87,6 +91,9 @@ def ref() -> ctypes.CDLL:
                                            ctypes.c_longlong, _D, _D, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]
+        lib.chaos_ref_dopri_trajectory.argtypes = [ctypes.c_char_p, _D, _D, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_double,
+                                                   ctypes.c_double, ctypes.c_int, _D, _D, _D]
         _ref = lib
     return _ref
 
@@ -146,6 +153,28 @@ def adaptive(model: str, params, inits, k, integrator="dverk65", gs="cgs", rtol=
     if rc:
         raise ValueError("oracle rejected the arguments")
     return out, st, steps
+
+
+def dopri_trajectory(model: str, p, x0, h0, hmax, atol, rtol, nsteps, source: str = "oracle"):
+    """The state alone under Dormand-Prince 5(4), one accepted step per entry
+    from time 0, as the reference's dopriStep is called.  source "oracle":
+    the C restatement; "reference": the reference's own dopriStep
+    (cuda/tools/dopri.dp.cpp:7-139).  Returns (times, step proposals, states),
+    one row per accepted step."""
+    p, x0 = _c(p), _c(x0)
+    n = x0.shape[0]
+    t = np.zeros(nsteps)
+    h = np.zeros(nsteps)
+    x = np.zeros((nsteps, n))
+    args = (p.ctypes.data_as(_D), x0.ctypes.data_as(_D), h0, hmax, atol, rtol, nsteps,
+            t.ctypes.data_as(_D), h.ctypes.data_as(_D), x.ctypes.data_as(_D))
+    if source == "reference":
+        rc = ref().chaos_ref_dopri_trajectory(model.encode(), *args)
+    else:
+        rc = orc().orc_dopri_trajectory(MODELS[model], *args)
+    if rc:
+        raise ValueError(f"{source} trajectory failed ({rc})")
+    return t, h, x
 
 
 def make_grid(m, base, s1, s2):

@@ -579,6 +579,10 @@ static int try_step(integ_t *s, double *y, double h, double *err_out) {
     }
     for (int st = 1; st < 7; st++) {
       for (int c = 0; c < N; c++) {
+        if (st == 1) { /* dopri.dp.cpp:71: val + step * a21 * k1, no parentheses */
+          arg[c] = y[c] + h * DP_A[1][0] * K[c];
+          continue;
+        }
         double acc = 0;
         for (int q = 0; q < st; q++) acc += DP_A[st][q] * K[q * N + c];
         arg[c] = y[c] + h * acc;
@@ -599,15 +603,44 @@ static int try_step(integ_t *s, double *y, double h, double *err_out) {
   return err <= 1.0;
 }
 
-/* Integrates y over exactly `len` time units.  Step-size control as in
- * cuda/tools/dopri.dp.cpp:46-138 (safety 0.9, fac1 0.2, fac2 10, beta 0.04,
- * exponent 1/q - 0.75 beta, q = 5 for Dopri5 and 6 for DVERK 6(5)).  A step
- * clamped to land on the end point does not shrink the proposal carried on.
- * Returns 0, or the status code of the failure. */
-static int integrate(integ_t *s, double *y, double len) {
+/* The step-size controller of cuda/tools/dopri.dp.cpp:46-138 after an
+ * attempted step of length h whose error norm is err: safety 0.9, the step
+ * shrinks by at most 1 / fac1 = 5 and grows by at most 1 / fac2 = 10, PI
+ * exponent expo1 = 1/q - 0.75 beta with beta = 0.04 (q = 5 for Dopri5, 6 for
+ * DVERK 6(5)), previous error floored at 1e-4, the step after a rejection no
+ * longer than the rejected one.  Returns 1 when the step is accepted (*hnext =
+ * the next proposal), 0 when it is rejected (*hnext = the retry length). */
+static int control(integ_t *s, double err, double h, double hmax, int *reject, double *hnext) {
   const double safe = 0.9, fac1 = 0.2, fac2 = 10., beta = 0.04;
   const double expo1 = (s->cfg->integrator == ORC_DVERK65 ? 1. / 6. : 0.2) - beta * 0.75;
   const double facc1 = 1. / fac1, facc2 = 1. / fac2;
+  double fac11 = pow(err, expo1);
+  double fac = fac11 / pow(s->fac_old, beta);
+  fac = fmax(facc2, fmin(facc1, fac / safe));
+  double hnew = h / fac;
+  if (err <= 1.0) {
+    s->fac_old = fmax(err, 1e-4);
+    if (hnew > hmax) hnew = hmax;
+    if (*reject) hnew = fmin(hnew, h);
+    *reject = 0;
+    *hnext = hnew;
+    return 1;
+  }
+  *reject = 1;
+  *hnext = h / fmin(facc1, fac11 / safe);
+  return 0;
+}
+
+/* Takes the attempted step: y <- y1 (and, for Dopri5, the FSAL derivative). */
+static void take_step(integ_t *s, double *y) {
+  memcpy(y, s->y1, sizeof(double) * s->N);
+  if (s->cfg->integrator == ORC_DOPRI5) memcpy(s->K, s->K + 6 * s->N, sizeof(double) * s->N);
+}
+
+/* Integrates y over exactly `len` time units with the controller above.  A
+ * step clamped to land on the end point does not shrink the proposal carried
+ * on.  Returns 0, or the status code of the failure. */
+static int integrate(integ_t *s, double *y, double len) {
   const double hmax = s->cfg->hmax > 0 ? s->cfg->hmax : 1e300;
   double t = 0;
   int reject = 0;
@@ -617,31 +650,54 @@ static int integrate(integ_t *s, double *y, double len) {
     double remaining = len - t;
     int clamped = s->h >= remaining;
     double h = clamped ? remaining : s->h;
-    double err;
+    double err, hnew;
     s->steps++;
-    int ok = try_step(s, y, h, &err);
+    try_step(s, y, h, &err);
     if (!isfinite(err)) return 1;
-    double fac11 = pow(err, expo1);
-    double fac = fac11 / pow(s->fac_old, beta);
-    fac = fmax(facc2, fmin(facc1, fac / safe));
-    double hnew = h / fac;
-    if (ok) {
-      s->fac_old = fmax(err, 1e-4);
-      memcpy(y, s->y1, sizeof(double) * s->N);
-      if (s->cfg->integrator == ORC_DOPRI5) memcpy(s->K, s->K + 6 * s->N, sizeof(double) * s->N);
-      if (hnew > hmax) hnew = hmax;
-      if (reject) hnew = fmin(hnew, h);
-      reject = 0;
+    if (control(s, err, h, hmax, &reject, &hnew)) {
+      take_step(s, y);
       t = clamped ? len : t + h;
       if (!clamped || hnew < h) s->h = hnew; /* else keep the unclamped proposal */
       if (s->cfg->escape > 0)
         for (int c = 0; c < s->n; c++)
           if (!(fabs(y[c]) <= s->cfg->escape)) return 4;
     } else {
-      hnew = h / fmin(facc1, fac11 / safe);
-      reject = 1;
       s->h = hnew;
     }
+  }
+  return 0;
+}
+
+int orc_dopri_trajectory(int model, const double *p, const double *x0, double h0, double hmax,
+                         double atol, double rtol, int nsteps, double *t_out, double *h_out,
+                         double *x_out) {
+  const int n = orc_model_dim(model);
+  if (n < 0 || orc_model_is_map(model) || nsteps < 0 || !(h0 > 0)) return -1;
+  orc_adaptive_cfg cfg = {model, 0, ORC_DOPRI5, ORC_CGS, rtol, atol, h0, hmax, 0.0,
+                          0.0, 0.0, 1.0, 1.0, INT64_MAX, 0.0};
+  double buf[12 * L96_N];
+  double *y = buf, *K = y + n, *y1 = K + 8 * n, *tmp = y1 + n;
+  integ_t s = {&cfg, n, 0, n, p, h0, 1e-4, 1, 0, 0, K, y1, tmp};
+  double t = 0;
+  memcpy(y, x0, sizeof(double) * n);
+  for (int i = 0; i < nsteps; i++) {
+    int reject = 0, ok = 0;
+    while (!ok) { /* one accepted step, rejected attempts retried */
+      const double h = s.h;
+      double err, hnew;
+      s.steps++;
+      try_step(&s, y, h, &err);
+      if (!isfinite(err)) return 1;
+      ok = control(&s, err, h, hmax, &reject, &hnew);
+      if (ok) {
+        take_step(&s, y);
+        t += h;
+      }
+      s.h = hnew;
+    }
+    t_out[i] = t;
+    h_out[i] = s.h;
+    memcpy(x_out + (size_t)i * n, y, sizeof(double) * n);
   }
   return 0;
 }

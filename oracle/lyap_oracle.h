@@ -58,6 +58,16 @@ int orc_lyap_adaptive(const orc_adaptive_cfg *cfg, int64_t P, const double *para
                       const double *inits, double *out, int32_t *status, int64_t *steps,
                       int threads);
 
+/* The state alone under Dormand-Prince 5(4) with the controller of the
+ * adaptive forms (cuda/tools/dopri.dp.cpp:46-138), stepped the way the
+ * reference's dopriStep is called: time from 0, one accepted step per entry
+ * (rejections retried), no end point to land on.  After step i: t_out[i] =
+ * time, h_out[i] = the next step's proposal, x_out[i*n..] = the state.
+ * Returns 0, 1 on a non-finite error norm, or -1 on bad arguments. */
+int orc_dopri_trajectory(int model, const double *p, const double *x0, double h0, double hmax,
+                         double atol, double rtol, int nsteps, double *t_out, double *h_out,
+                         double *x_out);
+
 /* Philox4x64-10 (Salmon et al., SC'11): out[4] = philox(ctr[4], key[2]). */
 void orc_philox4x64(const uint64_t ctr[4], const uint64_t key[2], uint64_t out[4]);
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "cuda/lyapunov.dp.hpp"
+#include "cuda/tools/dopri.dp.hpp"
 #include "singleton.h"
 
 namespace {
@@ -92,6 +93,40 @@ int chaos_ref_lyapunov(const char *name, int is_qr, int is_var, long long P, con
 
   std::memcpy(lyap_out, lyap.p, sizeof(double) * (size_t)P * k);
   std::memcpy(inits, ini.p, sizeof(double) * (size_t)P * n);
+  return 0;
+}
+
+// The reference's Dormand-Prince step, dopriStep (cuda/tools/dopri.dp.cpp:7-139),
+// driven over one state trajectory the way a caller of that tool drives it:
+// time starts at 0 (the first call sets facOld = 1e-4 and evaluates k1,
+// :65-68), each call makes one accepted step (rejected attempts are retried
+// inside the call, :133-138) and leaves the next step's proposal in `step` and
+// the FSAL derivative in k1.  After call i: t_out[i] = time, h_out[i] = step,
+// x_out[i*n .. i*n+n-1] = the state.  tolLocErr = atol, tolGlobErr = rtol
+// (error weights atol + rtol max(|y0|, |y1|), :98-104).  Returns 0, or -1 for
+// an unknown model / bad arguments.
+int chaos_ref_dopri_trajectory(const char *name, const double *params, const double *x0,
+                               double h0, double hmax, double atol, double rtol, int nsteps,
+                               double *t_out, double *h_out, double *x_out) {
+  auto &storage = Singleton<ModelFactoryRegistry::Storage>::Instance();
+  auto it = storage._data.find(name);
+  if (it == storage._data.end() || nsteps < 0 || !(h0 > 0)) return -1;
+  ModelFactoryRegistry::ModelData &md = it->second;
+  if (md._type != ModelType::flow) return -1;
+  const int n = md._dimension, m = md._param_number;
+  diffSysFunc f = nullptr;
+  md._model_func(&f);
+  std::vector<double> prm(params, params + m), x(x0, x0 + n), spare(n), ysti(n), arg(n), k1(n),
+      k2(n), k3(n), k4(n), k5(n), k6(n);
+  double step = h0, time = 0.0, fac_old = 0.0;
+  for (int i = 0; i < nsteps; i++) {
+    dopriStep(x.data(), n, f, prm.data(), step, hmax, atol, rtol, spare.data(), ysti.data(),
+              arg.data(), k1.data(), k2.data(), k3.data(), k4.data(), k5.data(), k6.data(), time,
+              fac_old);
+    t_out[i] = time;
+    h_out[i] = step;
+    std::memcpy(x_out + (size_t)i * n, x.data(), sizeof(double) * n);
+  }
   return 0;
 }
 

@@ -1,8 +1,8 @@
-"""Generates tests/golden/reference_fixed.npz from the reference's own
-sources built for the host (oracle/_ref/libchaos_ref.so; recipe in
-oracle/Makefile).  Run here, where the reference tree is available:
+"""Generates tests/golden/reference_fixed.npz and reference_dopri.npz from
+the reference's own sources built for the host (oracle/_ref/libchaos_ref.so;
+recipe in oracle/Makefile).  Run where the reference tree is available:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--only fixed|dopri|program]
 
 Each case is one model x method on a few seeded points with short phase
 times (for the map model, iteration counts; maps have no QR branch); the fixture stores the inputs, the spectra and the end states the
@@ -77,8 +77,40 @@ def program_outputs():
             shutil.rmtree(d)
 
 
-def main():
-    program_outputs()
+# Dormand-Prince trajectories through the reference's dopriStep
+# (cuda/tools/dopri.dp.cpp:7-139): model -> (params, x0, h0, hmax, rtol = atol,
+# accepted steps).  Regular and chaotic cells, two tolerances.
+DOPRI_CASES = {
+    "shimizu_6": ("shimizu", [0.75, 0.45], [0.1, 0.0, 0.0], 1e-2, 0.5, 1e-6, 500),
+    "lorenz_6": ("lorenz", [10.0, 28.0, 8.0 / 3.0], [1.0, 1.0, 1.0], 1e-2, 0.5, 1e-6, 500),
+    "lorenz_10": ("lorenz", [10.0, 28.0, 8.0 / 3.0], [1.0, 1.0, 1.0], 1e-3, 0.5, 1e-10, 500),
+    "rossler_6": ("rossler", [0.1, 0.2, 4.0], [1.0, 1.0, 0.0], 1e-2, 0.5, 1e-6, 500),
+    "chua_8": ("chua", [9.0, 14.3, -8.0 / 7.0, -5.0 / 7.0], [0.1, 0.0, 0.0], 1e-2, 0.5, 1e-8,
+               500),
+    "hyper_rossler_8": ("hyper_rossler", [0.5, 0.05], [-10.0, -6.0, 0.0, 10.0], 1e-2, 0.5, 1e-8,
+                        500),
+}
+
+
+def dopri_trajectories():
+    out = {}
+    for key, (model, p, x0, h0, hmax, tol, n) in DOPRI_CASES.items():
+        t, h, x = oracle.dopri_trajectory(model, p, x0, h0, hmax, tol, tol, n, source="reference")
+        out[key + "_cfg"] = np.array([h0, hmax, tol, n], dtype=float)
+        out[key + "_params"] = np.array(p, dtype=float)
+        out[key + "_x0"] = np.array(x0, dtype=float)
+        out[key + "_t"], out[key + "_h"], out[key + "_x"] = t, h, x
+    np.savez_compressed(os.path.join(HERE, "reference_dopri.npz"), **out)
+    print("wrote", len(out), "arrays (dopri)")
+
+
+def main(only=None):
+    if only in (None, "program"):
+        program_outputs()
+    if only in (None, "dopri"):
+        dopri_trajectories()
+    if only not in (None, "fixed"):
+        return
     out = {}
     for model, (pb, xb, k, h, ts, tc, tt, dn) in CASES.items():
         params, inits = case_inputs(model)
@@ -97,4 +129,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", choices=["fixed", "dopri", "program"], default=None)
+    main(ap.parse_args().only)

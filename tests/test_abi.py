@@ -94,3 +94,44 @@ def test_inputs_match_oracle(lib, orc):
     assert abs(g.std() - 0.01) < 3e-4
     # any point regenerates alone (counter-based)
     assert np.array_equal(lib.make_inits(3, 5, [1.0, 1.0, 0.0], 1e-3, "uniform", 1)[4], u[4] + [1.0, 1.0, 0.0])
+
+
+def test_batch_rejects_a_handle_in_two_segments(lib):
+    """Two segments of one handle would share its longest-first order buffer;
+    the batch entry points refuse them before touching a device (the handle
+    pointer is only compared, so a placeholder stands in for a real one)."""
+    from chaos_oneapi_b200 import native
+    placeholder = ctypes.create_string_buffer(64)
+    h = ctypes.addressof(placeholder)
+    segs = (native.Segment * 2)()
+    for i in range(2):
+        segs[i] = native.Segment(h, 4, 8, 8, 8, None, None, None)
+    for call in (lambda: native.lib.chaos_lyap_run_batch(segs, 2, None),
+                 lambda: native.lib.chaos_lyap_batch_graph_create(segs, 2,
+                                                                  ctypes.byref(ctypes.c_void_p()))):
+        assert call() == native.EINVAL
+        assert b"share a handle" in native.lib.chaos_lyap_last_error()
+
+
+@pytest.mark.parametrize("kw,code,text", [
+    (dict(model="henon", k=2), 3, b"maps are iterated"),
+    (dict(h=float("nan")), 1, b"h must be > 0"),
+    (dict(precision="compat", integrator="dverk"), 3, b"adaptive forms"),
+    (dict(model="lorenz96"), 3, b"3-4 dimensional"),
+])
+def test_no_alloc_batch_validates_like_create(lib, kw, code, text):
+    """The no-allocation batch entry checks each descriptor with the handle
+    path's rules, before any device work."""
+    from chaos_oneapi_b200 import native
+    so = ctypes.CDLL(native.LIB_PATH)
+    so.chaos_lyap_run_batch_static.argtypes = [ctypes.POINTER(native.Desc),
+                                               ctypes.POINTER(native.Segment), ctypes.c_int,
+                                               ctypes.c_void_p]
+    so.chaos_lyap_static_last_error.restype = ctypes.c_char_p
+    cfg = dict(model="lorenz", method="var", integrator="dopri5", precision="fp32",
+               t_avg=10.0, dt_renorm=1.0)
+    cfg.update(kw)
+    descs = (native.Desc * 1)(lib.SweepConfig(**cfg).to_desc())
+    segs = (native.Segment * 1)(native.Segment(None, 4, 8, 8, 8, None, None, None))
+    assert so.chaos_lyap_run_batch_static(descs, segs, 1, None) == code
+    assert text in so.chaos_lyap_static_last_error()

@@ -1,0 +1,127 @@
+"""Per-point failure statuses in every kernel form, on the GPU, by short
+device-side limits that a test runs out (nothing here faults a GPU): one
+point per status among ordinary points of the same warp --
+  1 non-finite: a NaN parameter;
+  2 step underflow: a stiff point (Rossler c = 1e5, Lorenz-96 gamma = 1e6)
+    whose steps must fall below h_min = 1e-4 (ordinary points need >= 0.02);
+  3 step budget: an averaging time of 1e6 against max_steps = 3e5;
+  4 escape: an orbit with no bounded attractor (Rossler a = 0.6), or a
+    Lorenz-96 state started outside the escape radius.
+Each failing point ends alone: the other points finish with status 0 and the
+spectra of a run in which the failing points are ordinary ones (up to the
+renormalisation moments, which the warp-voted Gram-Schmidt shares among the
+lanes of a warp)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BAD = {3: 1, 10: 2, 17: 3, 24: 4}  # point index -> expected status
+
+
+def _rossler(orc):
+    params = orc.make_grid(3, [0.2, 0.2, 5.7], [0, 0.1, 0.3, 8], [2, 4.0, 6.0, 8])
+    inits = orc.make_inits(3, params.shape[0], [1.0, 1.0, 0.0], 1e-3, 0, 3)
+    tavg = np.full(params.shape[0], 20.0)
+    bad_p, bad_t = params.copy(), tavg.copy()
+    bad_p[3, 0] = np.nan
+    bad_p[10, 2] = 1e5
+    bad_t[17] = 1e6
+    bad_p[24, 0] = 0.6
+    return (params, inits, tavg), (bad_p, inits, bad_t)
+
+
+KW = dict(model="rossler", method="var", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-4,
+          t_transient=5.0, t_avg=20.0, dt_renorm=1.0, max_steps=300_000)
+FORMS = [("fp32", "dopri5", "direct"), ("fp32", "dopri5", "persistent"),
+         ("fp32", "dopri5", "split"), ("fp32", "dopri5", "split_persistent"),
+         ("fp64", "dverk65", "direct"), ("fp64", "dverk65", "split")]
+TOL = {"fp32": 2e-4, "fp64": 1e-7}
+
+
+def _sweep(lib, torch, sw, inp):
+    p, x, t = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in inp)
+    P = p.shape[0]
+    spec = torch.zeros((P, sw.k), dtype=torch.float64, device="cuda")
+    st = torch.full((P,), -1, dtype=torch.int32, device="cuda")
+    sw.run(p, x, spec, st, t_avg=t)
+    sw.sync()
+    return spec.cpu().numpy(), st.cpu().numpy()
+
+
+def _check(clean, bad, tol):
+    (cs, cst), (bs, bst) = clean, bad
+    assert (cst == 0).all(), cst
+    for i, code in BAD.items():
+        assert bst[i] == code, (i, bst[i], code)
+        assert np.isnan(bs[i]).all()
+    good = np.ones(len(bst), bool)
+    good[list(BAD)] = False
+    assert (bst[good] == 0).all()
+    np.testing.assert_allclose(bs[good], cs[good], rtol=0, atol=tol)
+
+
+@pytest.mark.parametrize("prec,integ,schedule", FORMS)
+def test_statuses_one_lane_and_split(lib, orc, prec, integ, schedule):
+    import torch
+    clean, bad = _rossler(orc)
+    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, **KW) as sw:
+        _check(_sweep(lib, torch, sw, clean), _sweep(lib, torch, sw, bad), TOL[prec])
+
+
+@pytest.mark.parametrize("form", ["persistent", "split_persistent"])
+def test_statuses_batch(lib, orc, form):
+    """The same points as one segment of a mixed batch beside a clean Lorenz
+    segment, in the one-lane and the split batch kernels."""
+    import torch
+    clean, bad = _rossler(orc)
+    lp = orc.make_grid(3, [10.0, 28.0, 8.0 / 3.0], [0, 5, 20, 4], [1, 0, 200, 4])
+    lx = orc.make_inits(3, 16, [1.0, 1.0, 1.0], 1e-3, 0, 1)
+    kw = {k: v for k, v in KW.items() if k != "model"}
+    results = []
+    for inp in (clean, bad):
+        sw_r = lib.Sweep(model="rossler", precision="fp32", integrator="dopri5", schedule=form,
+                         **kw)
+        sw_l = lib.Sweep(model="lorenz", precision="fp32", integrator="dopri5", schedule=form,
+                         **kw)
+        parts = []
+        for sw, (p, x, t) in ((sw_r, inp), (sw_l, (lp, lx, np.full(16, 20.0)))):
+            d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (p, x, t)]
+            spec = torch.zeros((d[0].shape[0], 3), dtype=torch.float64, device="cuda")
+            st = torch.full((d[0].shape[0],), -1, dtype=torch.int32, device="cuda")
+            parts.append((sw, d[0], d[1], spec, st, None, d[2]))
+        lib.run_batch(parts)
+        torch.cuda.synchronize()
+        results.append([(pt[3].cpu().numpy(), pt[4].cpu().numpy()) for pt in parts])
+        sw_r.close()
+        sw_l.close()
+    _check(results[0][0], results[1][0], TOL["fp32"])
+    assert (results[1][1][1] == 0).all()  # the Lorenz segment is untouched
+    np.testing.assert_allclose(results[1][1][0], results[0][1][0], rtol=0, atol=TOL["fp32"])
+
+
+@pytest.mark.parametrize("schedule", ["direct", "persistent"])
+def test_statuses_lorenz96_warp(lib, orc, schedule):
+    """Warp per point (N = 40): 8 points, statuses at 1, 3, 5, 6."""
+    import torch
+    params = orc.make_grid(2, [8.0, 1.0], [0, 4.0, 6.0, 4], [1, 0.8, 1.0, 2])
+    inits = orc.make_inits(40, 8, [0.0] * 40, 0.01, 1, 3) + params[:, :1]
+    tavg = np.full(8, 5.0)
+    bp, bx, bt = params.copy(), inits.copy(), tavg.copy()
+    bp[1, 0] = np.nan
+    bp[3, 1] = 1e6
+    bt[5] = 1e6
+    bx[6] += 2e4
+    kw = dict(model="lorenz96", method="var", integrator="dopri5", precision="fp32", k=40,
+              gs="mgs", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-4, t_transient=2.0, t_avg=5.0,
+              dt_renorm=0.5, max_steps=50_000, schedule=schedule)
+    with lib.Sweep(**kw) as sw:
+        cs, cst = _sweep(lib, torch, sw, (params, inits, tavg))
+        bs, bst = _sweep(lib, torch, sw, (bp, bx, bt))
+    assert (cst == 0).all()
+    want = {1: 1, 3: 2, 5: 3, 6: 4}
+    for i, code in want.items():
+        assert bst[i] == code, (i, bst[i])
+    good = [i for i in range(8) if i not in want]
+    assert (bst[good] == 0).all()
+    np.testing.assert_allclose(bs[good], cs[good], rtol=0, atol=1e-4)

@@ -103,3 +103,35 @@ def test_lane_mgs_and_alignment_phase(driver, orc, prec):
     st, _, lam = _run(driver, model, prec, "dopri5+mgs", 1e-6, 1e-2, ts, ta, tt, dt, p, x0)
     assert st == 0
     np.testing.assert_allclose(lam, ref[0], rtol=0, atol=1e-4)
+
+
+@pytest.fixture(scope="module")
+def traj_driver(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not found")
+    out = str(tmp_path_factory.mktemp("traj") / "traj_driver")
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I" + os.path.join(ROOT, "include"), "-o", out,
+                    os.path.join(HERE, "host", "traj_driver.cu")], check=True, capture_output=True)
+    return out
+
+
+import trajectory_cases as tc  # noqa: E402
+
+
+@pytest.mark.parametrize("name", tc.cases())
+def test_host_trajectory_follows_reference_dopri(traj_driver, name):
+    """The sweep kernels' Dormand-Prince pass and FP64 controller
+    (trajectory.cuh: run_trajectory over adaptive.cuh's attempt / control),
+    compiled for the host, against trajectories of the reference's own
+    dopriStep: the same accepted steps and rejections, proposals, times and
+    states within rounding (bounds and their reason: trajectory_cases.py)."""
+    c = tc.case(name)
+    args = [traj_driver, c["model"], "fp64", "dopri5", repr(c["tol"]), repr(c["h0"]),
+            repr(c["hmax"]), str(c["nsteps"])] + [repr(float(v)) for v in c["params"]]
+    args += ["--"] + [repr(float(v)) for v in c["x0"]]
+    out = subprocess.run(args, check=True, capture_output=True, text=True).stdout.split("\n")
+    assert int(out[0]) == 0
+    rows = np.array([[float(v) for v in ln.split()] for ln in out[1:] if ln.strip()])
+    tc.assert_follows_reference(rows[:, 0], rows[:, 1], rows[:, 2:], c)

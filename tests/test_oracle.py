@@ -230,3 +230,44 @@ def test_dopri5_order_conditions():
 def test_tree_counts():
     by, _ = _trees(6)
     assert [len(by[n]) for n in range(1, 7)] == [1, 1, 2, 4, 9, 20]
+
+
+DOPRI_GOLDEN = os.path.join(HERE, "golden", "reference_dopri.npz")
+
+
+def _dopri_cases():
+    g = np.load(DOPRI_GOLDEN)
+    return sorted({k.rsplit("_", 1)[0] for k in g.files})
+
+
+@pytest.mark.parametrize("case", _dopri_cases())
+def test_dopri_trajectory_matches_reference_fixtures_bitwise(orc, case):
+    """The restatement's Dormand-Prince 5(4) and step-size controller against
+    trajectories the reference's own dopriStep (cuda/tools/dopri.dp.cpp:7-139)
+    produced: every accepted time, step proposal and state, bit for bit --
+    including the steps that follow a rejection."""
+    g = np.load(DOPRI_GOLDEN)
+    h0, hmax, tol, n = g[case + "_cfg"]
+    model = case.rsplit("_", 1)[0]
+    t, h, x = orc.dopri_trajectory(model, g[case + "_params"], g[case + "_x0"], h0, hmax, tol,
+                                   tol, int(n))
+    assert np.array_equal(t, g[case + "_t"]) and np.array_equal(h, g[case + "_h"])
+    assert np.array_equal(x, g[case + "_x"])
+
+
+@pytest.mark.skipif(not __import__("oracle").have_ref(), reason="reference build not present")
+@pytest.mark.parametrize("model,p,x0", [
+    ("shimizu", [0.75, 0.45], [0.1, 0.0, 0.0]),
+    ("lorenz", [10.0, 28.0, 8.0 / 3.0], [1.0, 1.0, 1.0]),
+    ("rossler", [0.2, 0.2, 5.7], [1.0, 1.0, 0.0]),
+    ("chua", [9.0, 14.3, -8.0 / 7.0, -5.0 / 7.0], [0.1, 0.0, 0.0]),
+    ("hyper_rossler", [0.5, 0.05], [-10.0, -6.0, 0.0, 10.0])])
+@pytest.mark.parametrize("tol", [1e-6, 1e-10])
+def test_dopri_trajectory_matches_live_reference_bitwise(orc, model, p, x0, tol):
+    """5000 accepted steps through the live reference build (at tolerance
+    1e-6, 190-370 of them come after a rejected attempt): the controller's constants, the PI step law, the
+    retry after a rejection and the FSAL derivative agree bit for bit."""
+    a = orc.dopri_trajectory(model, p, x0, 1e-2, 0.5, tol, tol, 5000)
+    b = orc.dopri_trajectory(model, p, x0, 1e-2, 0.5, tol, tol, 5000, source="reference")
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
