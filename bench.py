@@ -1,9 +1,19 @@
 """Throughput of the Lyapunov-spectrum sweep.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload rossler1024|lorenz64|lorenz1024|l96_256|batch256|surrogate]
+                    [--workload lorenz1024|rossler1024|lorenz64|l96_256|batch256|surrogate]
 
-Workload (default ``rossler1024``, the precision form): Rossler
+Default workload ``lorenz1024``: the precision form on a 1024 x 1024 Lorenz
+map (sigma in [5, 20] x rho in [0, 200], beta = 8/3, x0 = (1, 1, 1) +
+U(-1e-3, 1e-3) seeded per point; Dormand-Prince 5(4) with state and tangent
+in FP32, rtol = atol = 1e-6; FP64 Gram-Schmidt and compensated log sums;
+transient 100, averaging 1000, renormalisation every 1), with the plain
+FP64 DVERK 6(5) rtol 1e-10 sweep of the same map timed once in the same
+run (the time ratio is the precision form's target), both forms' errors
+against the FP64 rtol 1e-12 oracle on 1024 random cells, and the Rossler
+map below timed once beside it with its own accuracy sample.
+
+``rossler1024`` (the precision form's configuration): Rossler
 dx = -y - z, dy = x + a y, dz = b + z (x - c), b = 0.2, on a 1024 x 1024 grid
 a in [0.05, 0.45] x c in [2, 12]; x0 = (1, 1, 0) + U(-1e-3, 1e-3) seeded per
 point; Dormand-Prince 5(4) with state and tangent in FP32 (rtol = atol =
@@ -11,11 +21,7 @@ point; Dormand-Prince 5(4) with state and tangent in FP32 (rtol = atol =
 500, averaging 5000 time units, renormalisation every 2.  One step = the
 whole map.  ``lorenz64``: Lorenz 64 x 64, sigma in [5, 20] x rho in [0, 200],
 beta = 8/3, DVERK 6(5) FP64 rtol = atol = 1e-10, transient 100, averaging
-1000, renormalisation every 1.  ``lorenz1024``: the same Lorenz ranges on a
-1024 x 1024 grid in the precision form (FP32 Dopri5 rtol 1e-6, FP64
-renormalisation), with the plain FP64 DVERK 6(5) rtol 1e-10 sweep of the same
-map timed once in the same run; the line reports the time ratio and both
-forms' errors against the FP64 rtol 1e-12 oracle.
+1000, renormalisation every 1.
 
 Under torchrun each rank sweeps its own map (jitter seed = rank): weak
 scaling, no collective on the data path; the reported time is the maximum
@@ -66,7 +72,8 @@ WORKLOADS = {
         s2=[1, 0.0, 200.0, 1024], x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dopri5",
         precision="fp32", rtol=1e-6, atol=1e-6, h=1e-3, t_transient=100.0, t_avg=1000.0,
         dt_renorm=1.0, dtype="fp32", ref_h=1e-3, ref_cost=0.32,
-        plain=dict(integrator="dverk65", precision="fp64", rtol=1e-10, atol=1e-10)),
+        plain=dict(integrator="dverk65", precision="fp64", rtol=1e-10, atol=1e-10),
+        second="rossler1024"),
     # warp-per-point form: Lorenz-96, N = 40, full 40-exponent spectrum
     "l96_256": dict(
         model="lorenz96", base=[8.0, 1.0], s1=[0, 4.0, 16.0, 256], s2=[1, 0.5, 1.5, 256],
@@ -82,10 +89,18 @@ MODEL_FLOPS = {"rossler": (7, 8, 3), "lorenz": (9, 12, 3), "chua": (14, 9, 3),
 
 
 def flops_per_step(model, integrator, k=None):
+    """A step of the state and its k tangent vectors (averaging / alignment)."""
     S, C = STAGES[integrator]
     ff, fj, n = MODEL_FLOPS[model]
     k = n if k is None else k
     return S * (ff + k * fj) + 2 * C * n * (1 + k)
+
+
+def flops_per_state_step(model, integrator):
+    """A transient step: the state alone."""
+    S, C = STAGES[integrator]
+    ff, _, n = MODEL_FLOPS[model]
+    return S * ff + 2 * C * n
 
 
 class ClockSampler:
@@ -153,16 +168,31 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_inputs(w, seed):
-    import chaos_oneapi_b200 as cl
-    params = cl.make_grid(len(w["base"]), w["base"], w["s1"], w["s2"])
+def build_inputs(w, seed, src=None):
+    """The workload's grid and seeded initial states, built by the library
+    (src None) or, for the reference arm, by the oracle's restatement of the
+    same generators, so that process loads none of this library's code."""
+    if src is None:
+        import chaos_oneapi_b200 as cl
+
+        def grid(m, base, s1, s2):
+            return cl.make_grid(m, base, s1, s2)
+
+        def inits_of(n, P, b, amp, dist):
+            return cl.make_inits(n, P, b, amp, dist, seed)
+    else:
+        grid = src.make_grid
+
+        def inits_of(n, P, b, amp, dist):
+            return src.make_inits(n, P, b, amp, 0 if dist == "uniform" else 1, seed)
+    params = grid(len(w["base"]), w["base"], w["s1"], w["s2"])
     if w["x0"] == "F":  # Lorenz-96: x0 = F + N(0, amp^2) per component
-        n = cl.model_info(w["model"])["dim"]
-        inits = cl.make_inits(n, params.shape[0], [0.0] * n, w["amp"], "normal", seed)
+        n = w["k"]
+        inits = inits_of(n, params.shape[0], [0.0] * n, w["amp"], "normal")
         inits += params[:, :1]
     else:
-        inits = cl.make_inits(len(w["x0"]), params.shape[0], w["x0"], w["amp"],
-                              w.get("dist", "uniform"), seed)
+        inits = inits_of(len(w["x0"]), params.shape[0], w["x0"], w["amp"],
+                         w.get("dist", "uniform"))
     return params, inits
 
 
@@ -198,7 +228,8 @@ def run_reference_arm(a, w, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    params, inits = build_inputs(w, 0)
+    import oracle
+    params, inits = build_inputs(w, 0, src=oracle)
     # per step about 20 s of the host's threads
     sample = int(max(threads, min(4096, 20.0 * threads / ref_seconds_per_point(w))))
     for _ in range(a.warmup):
@@ -250,11 +281,13 @@ def run_surrogate_bench(a, rank, world, local):
     """--workload surrogate: a Lorenz (sigma, rho) map of --map-size^2 cells
     (sigma in [5, 20], rho in [0, 200]) refined by the MLP ensemble, against
     the plain FP64 sweep (DVERK 6(5) rtol 1e-10, transient 100, averaging
-    1000), whose full-map time is extrapolated from a timed random sample of
-    2^18 cells; regime agreement on 10,000 seeded held-out cells."""
+    1000) of the whole map, timed with CUDA events in one launch
+    (--plain-sample N instead extrapolates from a timed random sample of N
+    cells); regime agreement on 10,000 seeded held-out cells."""
     import torch
     import chaos_oneapi_b200 as cl
-    from chaos_oneapi_b200.surrogate import MapSpec, RefineConfig, plain_sweep, refine_map
+    from chaos_oneapi_b200.surrogate import (MapSpec, RefineConfig, lam_limit_of, plain_sweep,
+                                             refine_map)
     torch.cuda.set_device(local)
     n = a.map_size
     spec = MapSpec("lorenz", [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, n], [1, 0.0, 200.0, n],
@@ -266,16 +299,32 @@ def run_surrogate_bench(a, rank, world, local):
     rng = np.random.default_rng(a.held_out_seed)
     held = rng.choice(P, 10000, replace=False)
     truth, st = plain_sweep(sw, spec, held)
-    sample = rng.choice(P, min(P, 1 << 18), replace=False)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    plain_sweep(sw, spec, sample)
-    plain_est = (time.perf_counter() - t0) * P / sample.size
-    cfg = RefineConfig(steps0=6000, steps_round=4000, rounds=4, round_grid_step=max(1, n // 512),
-                       round_max_new=65536, rule=a.surrogate_rule,
+    if a.plain_sample > 0:  # extrapolated from a timed random sample
+        sample = rng.choice(P, min(P, a.plain_sample), replace=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain_sweep(sw, spec, sample)
+        plain_est = (time.perf_counter() - t0) * P / sample.size
+        plain_how = f"extrapolated from a timed random sample of {sample.size} cells"
+    else:  # the whole map in one launch
+        allc = np.arange(P)
+        dp = torch.from_numpy(spec.params(allc)).cuda()
+        dx = torch.from_numpy(spec.inits(allc)).cuda()
+        ds = torch.empty((P, sw.k), dtype=torch.float64, device="cuda")
+        dst = torch.empty(P, dtype=torch.int32, device="cuda")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        sw.run(dp, dx, ds, dst)
+        e1.record()
+        torch.cuda.synchronize()
+        plain_est = e0.elapsed_time(e1) * 1e-3
+        plain_how = f"the whole {n}x{n} map in one launch, CUDA events"
+        del dp, dx, ds, dst
+    cfg = RefineConfig(round_grid_step=max(1, n // 512), rule=a.surrogate_rule,
                        regime_conf=a.regime_conf, regime_std=a.regime_std)
+    cfg.lam_limit = lam_limit_of(cfg)
     if cfg.rule == "regime":
-        cfg.lam_limit = 0.005
         rule = (f"integrate where the ensemble's regime score r = tanh((lambda_1 - "
                 f"{cfg.regime_threshold}) / {cfg.regime_width}) is not confident "
                 f"(|mean r| < {cfg.regime_conf} or std r > {cfg.regime_std}), disagrees with "
@@ -326,7 +375,7 @@ def run_surrogate_bench(a, rank, world, local):
                                    "SiLU, BF16 mma.sync, FP32 accumulate, Adam 1e-3",
                        "rule": rule,
                        "rounds": cfg.rounds, "round_max_new": cfg.round_max_new},
-            "refined_s": refined, "plain_estimate_s": plain_est,
+            "refined_s": refined, "plain_s": plain_est, "plain_timing": plain_how,
             "refined_over_plain": refined / plain_est,
             "plain_fraction": info["plain_fraction"], "training_cells": info["training_cells"],
             "timings": info["timings"], "clocks": clk,
@@ -473,26 +522,13 @@ def run_batch_bench(a, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
-def accuracy_vs(spec, status, ref, rst):
-    """Per-exponent error of `spec` against the oracle's `ref` on the points
-    both integrated to the end (status 0)."""
-    ok = (rst == 0) & (status == 0)
-    d = np.abs(spec[ok] - ref[ok])
-    chaotic = ref[ok][:, 0] > 0.01
-    return {
-        "sample": int(len(status)), "compared": int(ok.sum()),
-        "status_agree": float((rst == status).mean()),
-        "frac_all_within_1e-3": float((d.max(axis=1) <= 1e-3).mean()),
-        "frac_within_1e-3_per_exponent": [float(x) for x in (d <= 1e-3).mean(axis=0)][:8],
-        "median_abs_err": [float(x) for x in np.median(d, axis=0)][:8],
-        "max_abs_err_regular": ([float(x) for x in d[~chaotic].max(axis=0)][:8]
-                                if (~chaotic).any() else None),
-        "frac_regular_within_1e-3": (float((d[~chaotic].max(axis=1) <= 1e-3).mean())
-                                     if (~chaotic).any() else None),
-        "chaotic_cells": int(chaotic.sum()),
-        "regime_sign_agreement": float((np.sign(spec[ok][:, 0] - 0.01) ==
-                                        np.sign(ref[ok][:, 0] - 0.01)).mean()),
-    }
+def resident_mb(w):
+    """Device bytes a sweep of workload w touches: params, inits, spectrum,
+    status and step counts."""
+    P = int(w["s1"][3] * w["s2"][3])
+    m, k = len(w["base"]), w.get("k", 3)
+    n = k if w["x0"] == "F" else len(w["x0"])
+    return int(round(P * (8 * (m + n + k) + 4 + 8) / 1e6))
 
 
 def config_of(a, w, extra=None):
@@ -502,75 +538,100 @@ def config_of(a, w, extra=None):
          "t_transient": w["t_transient"], "t_avg": w["t_avg"], "dt_renorm": w["dt_renorm"],
          "global_points": int(w["s1"][3] * w["s2"][3]) * a.gpus,
          "parallelism": f"points sharded: one map per rank x {a.gpus}",
-         "l2": "inputs 72 MB < L2; a 256 MB buffer is written between timed steps"}
+         "l2": f"inputs and outputs {resident_mb(w)} MB (< 126 MB L2); a 256 MB buffer is "
+               "written between timed steps"}
     if extra:
         c.update(extra)
     return c
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="rossler1024",
-                    choices=sorted(WORKLOADS) + ["batch256", "surrogate"])
-    ap.add_argument("--map-size", type=int, default=4096, help="surrogate workload: cells per side")
-    ap.add_argument("--batch-form", default="mixed", choices=["mixed", "split", "lane"],
-                    help="batch256: every segment one point per lane, every segment one point "
-                         "per group of four lanes, or mixed: the hyperchaotic Rossler segment "
-                         "(whose stiff points set the run's length) split, the others per lane")
-    ap.add_argument("--surrogate-rule", default="regime", choices=["regime", "spread"],
-                    help="surrogate: which cells the plain sweep integrates (see RefineConfig)")
-    ap.add_argument("--regime-conf", type=float, default=0.8,
-                    help="surrogate, regime rule: integrate where |mean r| is below this")
-    ap.add_argument("--regime-std", type=float, default=0.1,
-                    help="surrogate, regime rule: integrate where std r is above this")
-    ap.add_argument("--held-out-seed", type=int, default=7,
-                    help="surrogate: seed of the 10,000 held-out cells")
-    ap.add_argument("--dump", default="",
-                    help="surrogate: write the held-out cells' predictions and truth (npz)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--accuracy-sample", type=int, default=256)
-    ap.add_argument("--variant", type=int, default=-1,
-                    help="FP32 kernel register variant; -1 = autotune")
-    a = ap.parse_args()
-    w = WORKLOADS.get(a.workload)
+def transient_steps(sw, dp, dx, stream):
+    """Per-point attempted steps of the transient alone: the same sweep with
+    every averaging time cut to 1e-6 (one clamped step after the transient;
+    the transient does not depend on what follows it)."""
+    import torch
+    P = dp.shape[0]
+    tiny = torch.full((P,), 1e-6, dtype=torch.float64, device=dp.device)
+    spec = torch.empty((P, sw.k), dtype=torch.float64, device=dp.device)
+    st = torch.empty(P, dtype=torch.int32, device=dp.device)
+    steps = torch.empty(P, dtype=torch.int64, device=dp.device)
+    sw.run(dp, dx, spec, st, steps, t_avg=tiny, stream=stream)
+    stream.synchronize()
+    return np.maximum(steps.cpu().numpy() - 1, 0)
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    a.gpus = max(a.gpus, world)
 
-    if a.workload == "surrogate":
-        if a.impl == "reference":
-            if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  "the reference has no surrogate form"}))
-            return
-        if rank == 0:
-            run_surrogate_bench(a, rank, world, local)
-        return
-    if a.workload == "batch256":
-        if a.impl == "reference":
-            if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  "the reference has no batching form (one model per run)"}))
-            return
-        if world > 1:
-            from datetime import timedelta
-            import torch.distributed as dist
-            dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-        run_batch_bench(a, rank, world, local)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
-    if a.impl == "reference":
-        run_reference_arm(a, w, rank)
-        return
+def algorithmic_flops(model, integrator, k, steps, steps_transient):
+    """Sum over points of transient steps x (state step) + the rest x (joint step)."""
+    joint = np.maximum(steps - steps_transient, 0)
+    return (float(steps_transient.sum()) * flops_per_state_step(model, integrator) +
+            float(joint.sum()) * flops_per_step(model, integrator, k))
 
+
+def oracle_runs(w, params, inits, k, idx, form_rtol, form_integrator):
+    """The FP64 oracle on the sample cells: the reference answer (rtol 1e-12),
+    itself at rtol 1e-11 (its own reproducibility), and the form's method in
+    FP64 at the form's tolerance."""
+    import oracle
+    orc_rtol = w.get("oracle_rtol", 1e-12)
+    integ = "dverk65" if k <= 4 else "dopri5"
+    common = dict(gs=w.get("gs", "cgs"), t_transient=w["t_transient"], t_avg=w["t_avg"],
+                  dt_renorm=w["dt_renorm"])
+    out = {"truth": oracle.adaptive(w["model"], params[idx], inits[idx], k, integrator=integ,
+                                    rtol=orc_rtol, atol=orc_rtol, **common)[:2]}
+    if k <= 4:
+        out["self"] = oracle.adaptive(w["model"], params[idx], inits[idx], k, integrator=integ,
+                                      rtol=orc_rtol * 10, atol=orc_rtol * 10, **common)[:2]
+        out["method"] = oracle.adaptive(w["model"], params[idx], inits[idx], k,
+                                        integrator=form_integrator, rtol=form_rtol,
+                                        atol=form_rtol, **common)[:2]
+    return out
+
+
+def accuracy_vs(spec, status, ref, rst, others=None):
+    """Per-exponent error of `spec` against the oracle's `ref` on the points
+    both integrated to the end (status 0), split by regime (chaotic: the
+    oracle's lambda_1 > 0.01).  `others`: {name: (spec, status)} of the
+    oracle's own other runs on the same cells, reported the same way on the
+    regular cells, and the cells where they all agree with `ref` within 1e-3
+    ("conditioned": the finite-time exponents there do not depend on rounding
+    or on the tolerance)."""
+    ok = (rst == 0) & (status == 0)
+    d = np.abs(spec[ok] - ref[ok])
+    chaotic = ref[ok][:, 0] > 0.01
+    within = d.max(axis=1) <= 1e-3
+    out = {
+        "sample": int(len(status)), "compared": int(ok.sum()),
+        "status_agree": float((rst == status).mean()),
+        "frac_all_within_1e-3": float(within.mean()),
+        "frac_within_1e-3_per_exponent": [float(x) for x in (d <= 1e-3).mean(axis=0)][:8],
+        "median_abs_err": [float(x) for x in np.median(d, axis=0)][:8],
+        "regular_cells": int((~chaotic).sum()), "chaotic_cells": int(chaotic.sum()),
+        "frac_regular_within_1e-3": (float(within[~chaotic].mean())
+                                     if (~chaotic).any() else None),
+        "max_abs_err_regular": ([float(x) for x in d[~chaotic].max(axis=0)][:8]
+                                if (~chaotic).any() else None),
+        "frac_chaotic_within_1e-3": (float(within[chaotic].mean()) if chaotic.any() else None),
+        "regime_sign_agreement": float((np.sign(spec[ok][:, 0] - 0.01) ==
+                                        np.sign(ref[ok][:, 0] - 0.01)).mean()),
+    }
+    if others:
+        cond = ~chaotic
+        for name, (osp, ost) in others.items():
+            od = np.abs(osp[ok] - ref[ok]).max(axis=1)
+            good = (ost[ok] == 0) & (od <= 1e-3)
+            out[f"oracle_{name}_frac_regular_within_1e-3"] = (
+                float(good[~chaotic].mean()) if (~chaotic).any() else None)
+            cond = cond & good
+        out["conditioned_regular_cells"] = int(cond.sum())
+        out["frac_conditioned_within_1e-3"] = float(within[cond].mean()) if cond.any() else None
+    return out
+
+
+ORACLE_RUNS = {"self": "rtol x 10 (the oracle against itself)",
+               "method": "the form's integrator and tolerance in FP64"}
+
+
+def run_sweep_bench(a, w, rank, world, local):
     import torch
     import torch.distributed as dist
     import chaos_oneapi_b200 as cl
@@ -645,7 +706,8 @@ def main():
     steps_np = steps.cpu().numpy()
     status_np = st.cpu().numpy()
     spec_np = ds.cpu().numpy()
-    fl = float(steps_np.sum()) * flops_per_step(w["model"], w["integrator"], k)
+    steps_tr = transient_steps(sw, dp, dx, stream)
+    fl = algorithmic_flops(w["model"], w["integrator"], k, steps_np, steps_tr)
     achieved = fl / (kernel_ms * 1e-3) / 1e12
 
     # end to end: host buffers (pinned) through the C ABI's host path
@@ -696,9 +758,22 @@ def main():
             t = torch.tensor([plain_ms], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             plain_ms = t.item()
+        psteps_np = psteps.cpu().numpy()
+        psteps_tr = transient_steps(psw, dp, dx, stream)
+        pfl = algorithmic_flops(w["model"], w["plain"]["integrator"], k, psteps_np, psteps_tr)
+        ppeak = cl.fma_peak_tflops(local, w["plain"]["precision"], 1.0)
         psw.close()
+        pach = pfl / (plain_ms * 1e-3) / 1e12
         plain = {"ms": plain_ms, "launch": ptuned, "spec": pds.cpu().numpy(),
-                 "status": pst.cpu().numpy(), "steps": psteps.cpu().numpy()}
+                 "status": pst.cpu().numpy(), "steps": psteps_np,
+                 "roofline": {"bound": "fp64_fma", "achieved": pach, "peak": ppeak,
+                              "unit": "TFLOP/s", "frac": pach / ppeak}}
+
+    # the precision form's own map (Rossler 1024^2), timed once beside the
+    # headline workload, with its accuracy on a large sample
+    second = None
+    if a.with_rossler and w.get("second"):
+        second = run_second_map(a, WORKLOADS[w["second"]], cl, torch, dev, stream, flush, local)
 
     if rank != 0:
         if world > 1:
@@ -723,13 +798,17 @@ def main():
         "roofline": {"bound": "fp32_fma" if w["precision"] == "fp32" else "fp64_fma",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": "measured in-process (FMA-chain kernel, chaos_lyap_fma_peak)",
-                     "flops_per_step": flops_per_step(w["model"], w["integrator"], k),
+                     "peak_source": "measured in-process (FMA-chain kernel, chaos_lyap_fma_peak; "
+                                    "FP32: the faster of FFMA and packed FFMA2 chains)",
+                     "flops_per_joint_step": flops_per_step(w["model"], w["integrator"], k),
+                     "flops_per_transient_step": flops_per_state_step(w["model"],
+                                                                      w["integrator"]),
                      "kernel_ms": kernel_ms},
         "e2e": e2e,
         "points": {"ok": int((status_np == 0).sum()), "escaped": int((status_np == 4).sum()),
                    "other": int(((status_np != 0) & (status_np != 4)).sum()),
-                   "steps_mean": float(steps_np.mean()), "steps_max": int(steps_np.max())},
+                   "steps_mean": float(steps_np.mean()), "steps_max": int(steps_np.max()),
+                   "transient_steps_mean": float(steps_tr.mean())},
     }
 
     if plain is not None:
@@ -743,6 +822,7 @@ def main():
             "time_ratio_plain_over_form": plain["ms"] / form_ms,
             "plain_points_per_s": P * world / (plain["ms"] * 1e-3),
             "plain_steps_mean": float(plain["steps"].mean()),
+            "plain_roofline": plain["roofline"],
             "whole_map_vs_plain": {
                 "compared": int(both.sum()),
                 "status_agree": float((status_np == plain["status"]).mean()),
@@ -757,21 +837,20 @@ def main():
         line["trace_identity"] = {"points": int(okp.sum()), "median_abs": float(np.median(tr)),
                                   "max_abs": float(tr.max())}
     if a.accuracy_sample > 0:
-        import oracle
         rng = np.random.default_rng(1234)
         sample = a.accuracy_sample if k <= 4 else min(a.accuracy_sample, 16)
         idx = rng.choice(P, sample, replace=False)
+        runs = oracle_runs(w, params, inits, k, idx, w["rtol"], w["integrator"])
+        ref, rst = runs.pop("truth")
         orc_rtol = w.get("oracle_rtol", 1e-12)
-        ref, rst, _ = oracle.adaptive(w["model"], params[idx], inits[idx], k,
-                                      integrator="dverk65" if k <= 4 else "dopri5",
-                                      gs=w.get("gs", "cgs"), rtol=orc_rtol, atol=orc_rtol,
-                                      t_transient=w["t_transient"], t_avg=w["t_avg"],
-                                      dt_renorm=w["dt_renorm"])
         line["accuracy"] = dict(vs=f"FP64 adaptive oracle, rtol=atol={orc_rtol:g} (CPU)",
-                                **accuracy_vs(spec_np[idx], status_np[idx], ref, rst))
+                                oracle_runs=ORACLE_RUNS if runs else None,
+                                **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs))
         if plain is not None:
             line["vs_plain_fp64"]["accuracy"] = accuracy_vs(plain["spec"][idx],
                                                             plain["status"][idx], ref, rst)
+    if second is not None:
+        line["precision_form_" + w["second"]] = second
 
     if not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -784,6 +863,129 @@ def main():
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_second_map(a, w, cl, torch, dev, stream, flush, local):
+    """One timed sweep of workload `w` (after the autotuner and a warm-up) and
+    its accuracy against the FP64 oracle on a random sample of
+    --second-accuracy-sample cells, split by regime."""
+    params, inits = build_inputs(w, 0)
+    P = params.shape[0]
+    k = w.get("k", 3)
+    sw = cl.Sweep(model=w["model"], method="var", integrator=w["integrator"],
+                  precision=w["precision"], rtol=w["rtol"], atol=w["atol"], h=w["h"],
+                  t_transient=w["t_transient"], t_avg=w["t_avg"], dt_renorm=w["dt_renorm"],
+                  k=k, device=local, schedule="persistent")
+    dp = torch.from_numpy(params).to(dev)
+    dx = torch.from_numpy(inits).to(dev)
+    ds = torch.empty((P, k), dtype=torch.float64, device=dev)
+    st = torch.empty(P, dtype=torch.int32, device=dev)
+    steps = torch.empty(P, dtype=torch.int64, device=dev)
+    tuned = sw.autotune(dp, dx, sample=min(P, 1 << 17))
+    with torch.cuda.stream(stream):
+        sw.run(dp, dx, ds, st, steps, stream=stream)
+        flush.fill_(0x33)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sw.run(dp, dx, ds, st, steps, stream=stream)
+        e1.record(stream)
+        stream.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps_np, status_np, spec_np = steps.cpu().numpy(), st.cpu().numpy(), ds.cpu().numpy()
+    steps_tr = transient_steps(sw, dp, dx, stream)
+    fl = algorithmic_flops(w["model"], w["integrator"], k, steps_np, steps_tr)
+    peak = cl.fma_peak_tflops(local, "fp32" if w["precision"] == "fp32" else "fp64", 1.0)
+    sw.close()
+    out = {"workload": {key: w[key] for key in ("model", "integrator", "precision", "rtol",
+                                                 "t_transient", "t_avg", "dt_renorm")},
+           "grid": f"{int(w['s1'][3])}x{int(w['s2'][3])}", "launch": tuned,
+           "ms": ms, "points_per_s": P / (ms * 1e-3),
+           "roofline": {"achieved": fl / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                        "frac": fl / (ms * 1e-3) / 1e12 / peak},
+           "points": {"ok": int((status_np == 0).sum()), "escaped": int((status_np == 4).sum()),
+                      "steps_mean": float(steps_np.mean()),
+                      "transient_steps_mean": float(steps_tr.mean())}}
+    if a.second_accuracy_sample > 0:
+        rng = np.random.default_rng(4321)
+        idx = rng.choice(P, a.second_accuracy_sample, replace=False)
+        runs = oracle_runs(w, params, inits, k, idx, w["rtol"], w["integrator"])
+        ref, rst = runs.pop("truth")
+        out["accuracy"] = dict(vs="FP64 adaptive oracle, rtol=atol=1e-12 (CPU)",
+                               oracle_runs=ORACLE_RUNS,
+                               **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lorenz1024",
+                    choices=sorted(WORKLOADS) + ["batch256", "surrogate"])
+    ap.add_argument("--map-size", type=int, default=4096, help="surrogate workload: cells per side")
+    ap.add_argument("--batch-form", default="mixed", choices=["mixed", "split", "lane"],
+                    help="batch256: every segment one point per lane, every segment one point "
+                         "per group of four lanes, or mixed: the hyperchaotic Rossler segment "
+                         "(whose stiff points set the run's length) split, the others per lane")
+    ap.add_argument("--surrogate-rule", default="regime", choices=["regime", "spread"],
+                    help="surrogate: which cells the plain sweep integrates (see RefineConfig)")
+    ap.add_argument("--regime-conf", type=float, default=0.8,
+                    help="surrogate, regime rule: integrate where |mean r| is below this")
+    ap.add_argument("--regime-std", type=float, default=0.1,
+                    help="surrogate, regime rule: integrate where std r is above this")
+    ap.add_argument("--held-out-seed", type=int, default=7,
+                    help="surrogate: seed of the 10,000 held-out cells")
+    ap.add_argument("--dump", default="",
+                    help="surrogate: write the held-out cells' predictions and truth (npz)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-sample", type=int, default=1024)
+    ap.add_argument("--second-accuracy-sample", type=int, default=1024,
+                    help="lorenz1024: cells of the Rossler 1024^2 map checked against the oracle")
+    ap.add_argument("--no-rossler", dest="with_rossler", action="store_false",
+                    help="lorenz1024: skip the Rossler 1024^2 precision-form map timed beside it")
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="surrogate: time the plain sweep on this many random cells and "
+                         "extrapolate (0: time the whole map)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="FP32 kernel register variant; -1 = autotune")
+    a = ap.parse_args()
+    w = WORKLOADS.get(a.workload)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    a.gpus = max(a.gpus, world)
+
+    if a.workload == "surrogate":
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no surrogate form"}))
+            return
+        if rank == 0:
+            run_surrogate_bench(a, rank, world, local)
+        return
+    if a.workload == "batch256":
+        if a.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no batching form (one model per run)"}))
+            return
+        if world > 1:
+            from datetime import timedelta
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        run_batch_bench(a, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if a.impl == "reference":
+        run_reference_arm(a, w, rank)
+        return
+    run_sweep_bench(a, w, rank, world, local)
 
 
 if __name__ == "__main__":

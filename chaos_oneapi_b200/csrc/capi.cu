@@ -360,10 +360,13 @@ static int ensure_order(chaos_lyap_handle *h, int64_t P) {
   return CHAOS_LYAP_OK;
 }
 
+// P points of params / inits are read at every `stride`-th point of arrays
+// that hold P_full points (stride 1, P_full = 0: the arrays themselves); the
+// spectrum, status and steps arrays hold P points.
 static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double *inits,
                    double *spectrum, int32_t *status, int64_t *steps, const double *tavg,
                    cudaStream_t s, int block, int schedule, int variant, double t_avg_override,
-                   double t_transient_override) {
+                   double t_transient_override, int64_t P_full = 0, int64_t stride = 1) {
   const chaos_lyap_desc &d = h->d;
   const ModelInfo *m = h->model;
   int rc;
@@ -401,8 +404,10 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
     a.dt_renorm = d.dt_renorm;
     a.max_steps = d.max_steps;
     a.escape = d.escape > 0 ? d.escape : 1e4;
-    a.params = cview(params, P, m->nparams, d.layout);
-    a.inits = cview(inits, P, m->dim, d.layout);
+    a.params = cview(params, P_full > 0 ? P_full : P, m->nparams, d.layout);
+    a.inits = cview(inits, P_full > 0 ? P_full : P, m->dim, d.layout);
+    a.params.ps *= stride;
+    a.inits.ps *= stride;
     a.t_avg_per_point = t_avg_override > 0 ? nullptr : tavg;
     a.spectrum = view(spectrum, P, d.k, d.layout);
     a.status = status;
@@ -510,8 +515,11 @@ int chaos_lyap_run_host(chaos_lyap_handle *h, int64_t P, const double *params, d
   return CHAOS_LYAP_OK;
 }
 
-int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
-                        const double *inits, int32_t *block_out, int32_t *schedule_out) {
+// Times short runs of `sample` points -- every `stride`-th of the P_full
+// points of the arrays -- in every launch shape and keeps the fastest.
+static int autotune(chaos_lyap_handle *h, int64_t P_full, int64_t sample, int64_t stride,
+                    const double *params, const double *inits, int32_t *block_out,
+                    int32_t *schedule_out) {
   if (!h) return fail(CHAOS_LYAP_EINVAL, "handle is null");
   if (sample <= 0 || !params || !inits) return fail(CHAOS_LYAP_EINVAL, "bad sample");
   if (h->d.precision == CHAOS_PREC_COMPAT_FP64 || h->model->dim > 4) {
@@ -547,7 +555,7 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
         for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
           cudaEventRecord(e0, s);
           rc = enqueue(h, sample, params, const_cast<double *>(inits), spec, nullptr, nullptr,
-                       nullptr, s, b, sc, v, t_avg, t_tr);
+                       nullptr, s, b, sc, v, t_avg, t_tr, P_full, stride);
           cudaEventRecord(e1, s);
           cudaEventSynchronize(e1);
           cudaEventElapsedTime(&ms, e0, e1);  // second repetition is the warm one
@@ -570,6 +578,19 @@ int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *para
   if (block_out) *block_out = best_b;
   if (schedule_out) *schedule_out = best_s;
   return CHAOS_LYAP_OK;
+}
+
+int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
+                        const double *inits, int32_t *block_out, int32_t *schedule_out) {
+  return autotune(h, sample, sample, 1, params, inits, block_out, schedule_out);
+}
+
+int chaos_lyap_autotune_map(chaos_lyap_handle *h, int64_t P, int64_t sample,
+                            const double *params, const double *inits, int32_t *block_out,
+                            int32_t *schedule_out) {
+  if (P <= 0 || sample <= 0) return fail(CHAOS_LYAP_EINVAL, "P and sample must be > 0");
+  const int64_t n = std::min(P, sample);
+  return autotune(h, P, n, P / n, params, inits, block_out, schedule_out);
 }
 
 // A batch runs each segment in the form of its handle's schedule: segments

@@ -88,6 +88,9 @@ SIGNATURES = {
     "chaos_lyap_autotune": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P,
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
+    "chaos_lyap_autotune_map": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _P, _P,
+                                               ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.POINTER(ctypes.c_int32)]),
     "chaos_lyap_run_batch": (ctypes.c_int, [ctypes.POINTER(Segment), ctypes.c_int, _P]),
     "chaos_lyap_batch_graph_create": (ctypes.c_int, [ctypes.POINTER(Segment), ctypes.c_int,
                                                      ctypes.POINTER(_P)]),

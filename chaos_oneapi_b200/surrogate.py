@@ -190,16 +190,16 @@ class RefineConfig:
     train_grid: int = 128          # initial plain sweep: train_grid x train_grid
     ensemble: int = 4
     width: int = 128
-    steps0: int = 3000             # Adam steps on the initial data
-    steps_round: int = 1500        # fine-tuning steps per refinement round
+    steps0: int = 6000             # Adam steps on the initial data
+    steps_round: int = 4000        # fine-tuning steps per refinement round
     batch: int = 1024
     lr: float = 1e-3
     lr_phases: tuple = (1.0, 0.3, 0.1)  # lr multipliers over equal thirds of each fit
     feature_scale: float = 0.0     # > 0: Gaussian random frequencies of this std
                                    # (cycles over the map); 0: axis-aligned default
-    rounds: int = 2
+    rounds: int = 4
     round_grid_step: int = 8       # candidates: every k-th cell of the fine map
-    round_max_new: int = 32768     # cells integrated per refinement round
+    round_max_new: int = 65536     # cells integrated per refinement round
     # Which cells the plain sweep integrates.  "spread": the ensemble's std
     # of lambda_1 above std_limit or the predicted |lambda_1| below
     # lam_limit.  "regime": the networks also learn a regime score
@@ -208,9 +208,13 @@ class RefineConfig:
     # is not confident (|mean r| < regime_conf or std r > regime_std) or
     # disagrees with the sign of its own mean lambda_1 - regime_threshold, or
     # where the predicted lambda_1 lies within lam_limit of the threshold.
-    rule: str = "spread"
+    # The defaults are the measured operating point: the regime rule at
+    # (0.8, 0.1), 4 rounds of up to 65,536 cells.
+    rule: str = "regime"
     std_limit: float = 0.02        # ensemble std of lambda_1
-    lam_limit: float = 0.05        # predicted |lambda_1| ("spread"); |lambda_1 - thr| ("regime")
+    # predicted |lambda_1| ("spread"; None: 0.05) or |lambda_1 - thr|
+    # ("regime"; None: 0.005)
+    lam_limit: float | None = None
     regime_threshold: float = 0.01
     regime_width: float = 0.005
     regime_conf: float = 0.8
@@ -237,15 +241,22 @@ def plain_sweep(sweep: Sweep, spec: MapSpec, index: np.ndarray, chunk: int = 1 <
     return spec_out, status
 
 
+def lam_limit_of(cfg) -> float:
+    """RefineConfig.lam_limit, or the rule's default when it is None."""
+    if cfg.lam_limit is not None:
+        return cfg.lam_limit
+    return 0.005 if cfg.rule == "regime" else 0.05
+
+
 def _flags(mean, std, cfg):
     if cfg.rule == "spread":
-        return (std[:, 0] > cfg.std_limit) | (mean[:, 0].abs() < cfg.lam_limit)
+        return (std[:, 0] > cfg.std_limit) | (mean[:, 0].abs() < lam_limit_of(cfg))
     if cfg.rule != "regime":
         raise ValueError(f"unknown rule {cfg.rule!r}")
     r, rs = mean[:, -1], std[:, -1]
     lam = mean[:, 0] - cfg.regime_threshold
     return ((r.abs() < cfg.regime_conf) | (rs > cfg.regime_std) | ((r > 0) != (lam > 0))
-            | (lam.abs() < cfg.lam_limit))
+            | (lam.abs() < lam_limit_of(cfg)))
 
 
 def _targets(y, cfg):

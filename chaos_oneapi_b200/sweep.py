@@ -200,11 +200,14 @@ class Sweep:
         return (spec, status, steps) if want_steps else (spec, status)
 
     def autotune(self, params, inits, sample: int | None = None):
-        P = params.shape[0]
+        """Picks the launch shape on `sample` points spread evenly over the map
+        (chaos_lyap_autotune_map) and keeps it in the handle."""
+        P = params.shape[0] if self.cfg.layout == "point" else params.shape[-1]
         sample = min(P, sample or 4096)
         b, s = ctypes.c_int32(), ctypes.c_int32()
-        check(lib.chaos_lyap_autotune(self._h, sample, _tptr(params, "float64"),
-                                      _tptr(inits, "float64"), ctypes.byref(b), ctypes.byref(s)))
+        check(lib.chaos_lyap_autotune_map(self._h, P, sample, _tptr(params, "float64"),
+                                          _tptr(inits, "float64"), ctypes.byref(b),
+                                          ctypes.byref(s)))
         return {"block": b.value, "schedule": {1: "direct", 2: "persistent", 3: "split", 4: "split_persistent"}.get(s.value, "auto"),
                 "variant": self.variant_in_use()}
 

@@ -182,6 +182,13 @@ int chaos_lyap_sync(chaos_lyap_handle *h);
 int chaos_lyap_autotune(chaos_lyap_handle *h, int64_t sample, const double *params,
                         const double *inits, int32_t *block_out, int32_t *schedule_out);
 
+/* The same over a whole map of P points: the sample is every (P / sample)-th
+ * point, spread over the map instead of its first rows (a map's cost varies
+ * across it: chaotic bands, escaping corners). */
+int chaos_lyap_autotune_map(chaos_lyap_handle *h, int64_t P, int64_t sample,
+                            const double *params, const double *inits, int32_t *block_out,
+                            int32_t *schedule_out);
+
 /* ---------------------------------------------------------- mixed batches
  * Several sweeps (segments: different 3- or 4-dimensional models, each with
  * its own handle, arrays and phase times; per-point averaging times allowed)
@@ -298,8 +305,9 @@ int chaos_lyap_make_inits(int32_t dim, int64_t P, const double *base, double amp
 
 /* Measures the FP32 (precision = CHAOS_PREC_FP32) or FP64 (CHAOS_PREC_FP64)
  * fused-multiply-add throughput of `device` with a kernel of independent FMA
- * chains running for about `seconds`; the roofline denominator of the sweep
- * kernels, which are bound by the FMA pipe.  No reference counterpart (the
+ * chains running for about `seconds` (FP32: the faster of scalar FFMA and
+ * packed FFMA2 chains); the roofline denominator of the sweep kernels, which
+ * are bound by the FMA pipe.  No reference counterpart (the
  * reference reports whole-run wall time only, raiitimer.h). */
 int chaos_lyap_fma_peak(int device, int precision, double seconds, double *tflops);
 

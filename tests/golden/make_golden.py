@@ -1,12 +1,14 @@
-"""Generates tests/golden/reference_fixed.npz and reference_dopri.npz from
-the reference's own sources built for the host (oracle/_ref/libchaos_ref.so;
-recipe in oracle/Makefile).  Run where the reference tree is available:
+"""Generates tests/golden/reference_fixed.npz, reference_dopri.npz and
+reference_config1.npz from the reference's own sources built for the host
+(oracle/_ref/libchaos_ref.so; recipe in oracle/Makefile).  Run where the
+reference tree is available:
 
-    python tests/golden/make_golden.py [--only fixed|dopri|program]
+    python tests/golden/make_golden.py [--only fixed|dopri|program|config1]
 
 Each case is one model x method on a few seeded points with short phase
-times (for the map model, iteration counts; maps have no QR branch); the fixture stores the inputs, the spectra and the end states the
-reference produced.
+times (for the map model, iteration counts; maps have no QR branch); the
+fixture stores the inputs, the spectra and the end states the reference
+produced.
 """
 import os
 import sys
@@ -104,11 +106,35 @@ def dopri_trajectories():
     print("wrote", len(out), "arrays (dopri)")
 
 
+# The 64 x 64 Lorenz map of the plain FP64 sweep (sigma in [5, 20], rho in
+# [0, 200], x0 = (1, 1, 1) + U(-1e-3, 1e-3) seed 0, transient 100, average
+# 1000, renormalisation every 1): eight of its regular cells -- six on a
+# stable fixed point, two on a periodic orbit -- through the reference's own
+# VAR method (cuda/lyapunov.dp.cpp:133-226) at a fixed step of 1e-4, the
+# yardstick of the adaptive FP64 sweep on the same cells.
+CONFIG1_CELLS = [325, 327, 1281, 2632, 2817, 3650, 1395, 1279]
+
+
+def config1_cells():
+    params = oracle.make_grid(3, [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, 64], [1, 0.0, 200.0, 64])
+    inits = oracle.make_inits(3, params.shape[0], [1.0, 1.0, 1.0], 1e-3, 0, 0)
+    idx = np.array(CONFIG1_CELLS)
+    h = 1e-4
+    spec, _ = oracle.reference("lorenz", "var", params[idx], inits[idx], 1e-7, h, 3, 100.0, 0.0,
+                               1000.0, 1.0 / h, threads=8)
+    np.savez_compressed(os.path.join(HERE, "reference_config1.npz"), index=idx,
+                        params=params[idx], inits=inits[idx], spectrum=spec,
+                        cfg=np.array([h, 100.0, 0.0, 1000.0, 1.0]))
+    print("wrote reference_config1.npz")
+
+
 def main(only=None):
     if only in (None, "program"):
         program_outputs()
     if only in (None, "dopri"):
         dopri_trajectories()
+    if only in (None, "config1"):
+        config1_cells()
     if only not in (None, "fixed"):
         return
     out = {}
@@ -131,5 +157,5 @@ def main(only=None):
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["fixed", "dopri", "program"], default=None)
+    ap.add_argument("--only", choices=["fixed", "dopri", "program", "config1"], default=None)
     main(ap.parse_args().only)

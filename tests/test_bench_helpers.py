@@ -31,3 +31,38 @@ def test_workloads_are_well_formed():
         assert w["s1"][3] > 1 and w["s2"][3] > 1, name
         assert w["integrator"] in bench.STAGES and w["model"] in bench.MODEL_FLOPS, name
         assert w["t_avg"] > 0 and w["dt_renorm"] > 0, name
+
+
+def test_transient_steps_count_as_state_steps():
+    # a transient step integrates the state alone: S F_f + 2 C n
+    assert bench.flops_per_state_step("rossler", "dopri5") == 6 * 7 + 2 * 26 * 3 == 198
+    steps = np.array([100, 50])
+    tr = np.array([40, 50])
+    want = 90 * 198 + 60 * 810
+    assert bench.algorithmic_flops("rossler", "dopri5", 3, steps, tr) == want
+
+
+def test_accuracy_summary_against_the_oracles_own_runs():
+    ref = np.array([[0.0, -0.1, -3.0], [-0.5, -1.0, -2.0], [0.0, -0.2, -4.0], [0.9, 0.0, -9.0]])
+    rst = np.zeros(4, dtype=np.int32)
+    spec = ref + np.array([[2e-3, 0, 0], [1e-4, 0, 0], [0, 0, 5e-4], [0, 0, 1e-2]])
+    # the oracle at another tolerance misses cell 0 as well: it is not conditioned
+    other = ref + np.array([[3e-3, 0, 0], [0, 0, 0], [0, 0, 0], [0, 0, 0]])
+    a = bench.accuracy_vs(spec, rst, ref, rst, {"self": (other, rst)})
+    assert a["regular_cells"] == 3 and a["chaotic_cells"] == 1
+    assert abs(a["frac_regular_within_1e-3"] - 2 / 3) < 1e-12
+    assert abs(a["oracle_self_frac_regular_within_1e-3"] - 2 / 3) < 1e-12
+    assert a["conditioned_regular_cells"] == 2 and a["frac_conditioned_within_1e-3"] == 1.0
+    assert a["frac_chaotic_within_1e-3"] == 0.0
+
+
+def test_reference_arm_inputs_come_from_the_oracle():
+    import oracle
+    w = bench.WORKLOADS["lorenz64"]
+    p1, x1 = bench.build_inputs(w, 3, src=oracle)
+    p2, x2 = bench.build_inputs(w, 3)
+    assert np.array_equal(p1, p2) and np.array_equal(x1, x2)
+    w = bench.WORKLOADS["l96_256"]
+    p1, x1 = bench.build_inputs(w, 1, src=oracle)
+    p2, x2 = bench.build_inputs(w, 1)
+    assert np.array_equal(p1, p2) and np.array_equal(x1, x2)

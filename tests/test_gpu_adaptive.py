@@ -88,3 +88,58 @@ def test_fp32_rossler_vs_fp64_oracle(lib, orc):
     # (lambda3 of a chaotic Rossler cell carries <x> over the window, whose
     # 200-unit average scatters by ~0.5 between nearby orbits)
     assert err[:, 0].max() < 0.05 and err[:, 1].max() < 0.05 and err.max() < 1.0, err.max(axis=0)
+
+
+@pytest.mark.parametrize("schedule", ["direct", "split"])
+def test_plain_fp64_sweep_matches_reference_config1_cells(lib, schedule):
+    """The plain FP64 sweep (DVERK 6(5), rtol = atol = 1e-10) of the 64 x 64
+    Lorenz map against the reference's own VAR method at a fixed step of
+    1e-4 on eight of its regular cells (tests/golden/reference_config1.npz,
+    written by the reference's sources): within 1e-4 on every exponent --
+    the FP64 path's correctness bar -- and, on the six fixed-point cells,
+    within 1e-7 (the FP64 oracle lands within 1e-9 there and within 5e-6 on
+    the two periodic cells)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_config1.npz"))
+    got, st, _ = _run(lib, "lorenz", g["params"], g["inits"], method="var", precision="fp64",
+                      integrator="dverk65", rtol=1e-10, atol=1e-10, h=1e-3, t_transient=100.0,
+                      t_avg=1000.0, dt_renorm=1.0, schedule=schedule)
+    assert (st == 0).all()
+    want = g["spectrum"]
+    assert np.abs(got - want).max() <= 1e-4, np.abs(got - want).max(axis=1)
+    fixed_point = want[:, 0] < -0.01
+    assert fixed_point.sum() == 6
+    assert np.abs(got - want)[fixed_point].max() <= 1e-7, np.abs(got - want).max(axis=1)
+
+
+@pytest.mark.parametrize("prec,integ,tol", [("fp64", "dverk65", 1e-6), ("fp32", "dopri5", 2e-4)])
+def test_autotuned_handle_matches_untuned(lib, orc, prec, integ, tol):
+    """Whatever launch shape the autotuner picks (block, one lane or four
+    lanes per point, direct or work queue, register variant), the spectra
+    are those of the untuned handle on cells that settle, within the
+    tolerance of the form (only the renormalisation moments, shared per warp,
+    differ)."""
+    import torch
+    params = orc.make_grid(3, [10.0, 28.0, 8.0 / 3.0], [0, 5, 20, 16], [1, 2, 20, 16])
+    P = params.shape[0]
+    inits = orc.make_inits(3, P, [1.0, 1.0, 1.0], 1e-3, 0, 2)
+    kw = dict(model="lorenz", method="var", integrator=integ, precision=prec, h=1e-3,
+              rtol=1e-10 if prec == "fp64" else 1e-6, atol=1e-10 if prec == "fp64" else 1e-6,
+              t_transient=20.0, t_avg=40.0, dt_renorm=1.0, schedule="persistent")
+    dp = torch.from_numpy(params).cuda()
+    dx = torch.from_numpy(inits).cuda()
+    out = []
+    for tune in (False, True):
+        with lib.Sweep(**kw) as sw:
+            if tune:
+                choice = sw.autotune(dp, dx, sample=64)
+                assert choice["block"] in (64, 128)
+            ds = torch.zeros((P, 3), dtype=torch.float64, device="cuda")
+            st = torch.full((P,), -1, dtype=torch.int32, device="cuda")
+            sw.run(dp, dx, ds, st)
+            sw.sync()
+            out.append((ds.cpu().numpy(), st.cpu().numpy()))
+    (a, sa), (b, sb) = out
+    assert (sa == 0).all() and (sb == 0).all()
+    assert a[:, 0].max() < -0.01  # every cell settles on a fixed point
+    np.testing.assert_allclose(b, a, rtol=0, atol=tol)
