@@ -64,14 +64,14 @@ WORKLOADS = {
         model="lorenz", base=[10.0, 28.0, 8.0 / 3.0], s1=[0, 5.0, 20.0, 64], s2=[1, 0.0, 200.0, 64],
         x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dverk65", precision="fp64", rtol=1e-10,
         atol=1e-10, h=1e-3, t_transient=100.0, t_avg=1000.0, dt_renorm=1.0, dtype="fp64",
-        ref_h=1e-3, ref_cost=0.32),
+        ref_h=1e-3),
     # precision form on the Lorenz map: FP32 Dopri5 against the plain FP64
     # DVERK 6(5) sweep of the same 1024^2 map, timed in the same run
     "lorenz1024": dict(
         model="lorenz", base=[10.0, 28.0, 8.0 / 3.0], s1=[0, 5.0, 20.0, 1024],
         s2=[1, 0.0, 200.0, 1024], x0=[1.0, 1.0, 1.0], amp=1e-3, integrator="dopri5",
         precision="fp32", rtol=1e-6, atol=1e-6, h=1e-3, t_transient=100.0, t_avg=1000.0,
-        dt_renorm=1.0, dtype="fp32", ref_h=1e-3, ref_cost=0.32,
+        dt_renorm=1.0, dtype="fp32", ref_h=1e-3,
         plain=dict(integrator="dverk65", precision="fp64", rtol=1e-10, atol=1e-10),
         second="rossler1024"),
     # warp-per-point form: Lorenz-96, N = 40, full 40-exponent spectrum
@@ -406,10 +406,13 @@ def run_batch_bench(a, rank, world, local):
         split = a.batch_form == "split" or (a.batch_form == "mixed" and name == "hyper_rossler")
         return "split_persistent" if split else "persistent"
     for name, seg in BATCH.items():
-        params = cl.make_grid(len(seg["base"]), seg["base"], seg["s1"], seg["s2"])
+        s1, s2 = seg["s1"], seg["s2"]
+        if a.grid > 0:
+            s1, s2 = s1[:3] + [a.grid], s2[:3] + [a.grid]
+        params = cl.make_grid(len(seg["base"]), seg["base"], s1, s2)
         P = params.shape[0]
         inits = cl.make_inits(len(seg["x0"]), P, seg["x0"], 1e-3, "uniform", rank)
-        tavg = rng.uniform(1000.0, 10000.0, P)
+        tavg = rng.uniform(1000.0, 10000.0, P) * a.t_scale
         sw = cl.Sweep(model=name, device=local, schedule=form_of(name), **BATCH_KW)
         sweeps.append(sw)
         direct.append(cl.Sweep(model=name, device=local, schedule="direct", **BATCH_KW))
@@ -500,7 +503,10 @@ def run_batch_bench(a, rank, world, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (seeded grids, jitter and averaging times)",
             "config": {"workload": "batch256", "segments": list(BATCH),
-                       "points_per_step": total_points, "t_avg": "U[1000, 10000] per point",
+                       "grid_per_segment": (f"{a.grid}x{a.grid}" if a.grid > 0 else "256x256"),
+                       "points_per_step": total_points,
+                       "t_avg": (f"U[1000, 10000] x {a.t_scale:g} per point" if a.t_scale != 1.0
+                                 else "U[1000, 10000] per point"),
                        **{k: v for k, v in BATCH_KW.items() if k != "t_avg"},
                        "launch": "one persistent batch kernel per step, replayed CUDA graph",
                        "form": {name: ("one point per group of four lanes"
@@ -659,6 +665,10 @@ def run_sweep_bench(a, w, rank, world, local):
     stream = torch.cuda.Stream(dev)
     if k > 4:  # warp-per-point kernel: one shape
         tuned = {"block": 256, "schedule": "persistent", "layout": "warp per point"}
+    elif forced_launch(a):
+        sw.close()
+        sw = cl.Sweep(**dict(common, **forced_launch(a)))
+        tuned = dict(forced_launch(a), how="forced (--launch)")
     elif a.variant < 0:
         tuned = sw.autotune(dp, dx, sample=min(P, 1 << 17))
     else:
@@ -916,6 +926,33 @@ def run_second_map(a, w, cl, torch, dev, stream, flush, local):
     return out
 
 
+def apply_overrides(a, w):
+    """--grid / --t-scale / --form on a copy of workload w."""
+    if a.grid > 0:
+        w["s1"] = w["s1"][:3] + [a.grid]
+        w["s2"] = w["s2"][:3] + [a.grid]
+        w.pop("second", None)
+    if a.t_scale != 1.0:
+        w["t_transient"] *= a.t_scale
+        w["t_avg"] *= a.t_scale
+        w.pop("second", None)
+    if a.form:
+        integ, prec, rtol = a.form.split(",")
+        w.update(integrator=integ, precision=prec, rtol=float(rtol), atol=float(rtol),
+                 dtype=prec)
+        w.pop("plain", None)
+        w.pop("second", None)
+    return w
+
+
+def forced_launch(a):
+    """--launch as Sweep keyword arguments, or None."""
+    if not a.launch:
+        return None
+    b, sched, var = a.launch.split(",")
+    return dict(block=int(b), schedule=sched, variant=int(var))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -950,8 +987,20 @@ def main():
                          "extrapolate (0: time the whole map)")
     ap.add_argument("--variant", type=int, default=-1,
                     help="FP32 kernel register variant; -1 = autotune")
+    # smaller cases of the same kernels (profiler captures, quick checks)
+    ap.add_argument("--grid", type=int, default=0, help="cells per side instead of the workload's")
+    ap.add_argument("--t-scale", type=float, default=1.0,
+                    help="scale the transient and averaging times (batch: the drawn times)")
+    ap.add_argument("--form", default="",
+                    help="integrator,precision,rtol instead of the workload's (e.g. "
+                         "dverk65,fp64,1e-10); drops the plain-sweep comparison")
+    ap.add_argument("--launch", default="",
+                    help="block,schedule,variant instead of the autotuner's choice "
+                         "(e.g. 128,direct,0; schedule direct|persistent|split|split_persistent)")
     a = ap.parse_args()
     w = WORKLOADS.get(a.workload)
+    if w is not None:
+        w = apply_overrides(a, dict(w))
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -7,7 +7,7 @@
 //             sin / cos (pi j u), sin / cos (pi j v), j = 1..4)
 //   network:  16 -> W -> W -> W -> 3 (W = 128), SiLU between layers
 //   numerics: weights and activations in BF16 for the tensor-core products
-//             (mma.sync m16n8k16, FP32 accumulate); FP32 master weights, FP32
+//             (tcgen05.mma, FP32 accumulate in tensor memory); FP32 master weights, FP32
 //             pre-activations for the backward pass, FP32 Adam moments
 //
 // All E networks advance together: every kernel takes the network index from
@@ -45,9 +45,28 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 // ------------------------------------------------------------------- GEMM
 // C[z](m, n) = sum_k A[z](m, k) B[z](k, n), A and B in BF16 at arbitrary
-// strides, C in FP32 (row-major, ldc).  64 x 64 tile per block, 4 warps of
-// 32 x 32, k in steps of 16 staged through shared memory so that the
-// fragments of mma.sync.m16n8k16 are contiguous pairs.
+// strides, C in FP32 (row-major, ldc), on the 5th-generation tensor cores:
+//
+//  * one CTA (4 warps) per 128-row x BN-column tile of C (BN = N rounded up to
+//    a multiple of 16, at most 128; blockIdx.z = the network);
+//  * K in blocks of 64: all threads gather the A block (128 x 64) and the B
+//    block (BN x 64, i.e. B^T, K-major) from global memory into shared memory
+//    in the tensor core's no-swizzle K-major layout -- 8 x 8 "core matrices"
+//    of 128 contiguous bytes, core matrices adjacent in K 128 bytes apart
+//    (the descriptor's leading byte offset), adjacent in M / N 1024 bytes
+//    apart (its stride byte offset); rows beyond M / N and k beyond K are
+//    zero.  Two shared-memory stages: the next block is gathered while the
+//    tensor core works on the current one;
+//  * one thread issues tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = BN,
+//    K = 16, BF16 x BF16 -> FP32) per 16-wide slice of the block, with the
+//    accumulator in tensor memory (TMEM, 128 columns allocated per CTA), and
+//    tcgen05.commit onto the stage's mbarrier, which the threads wait on
+//    before they overwrite that stage;
+//  * epilogue: each warp reads its 32 accumulator rows from TMEM
+//    (tcgen05.ld 32x32b, 16 columns at a time) and writes C (or adds to it).
+// No TMA: operands are gathered with ordinary loads, so any strides work
+// (the same kernel computes X W, A^T dZ and dZ W^T).  Every wait is bounded:
+// a wait that gives up sets *err and the kernel still frees its TMEM.
 struct GemmArgs {
   int M, N, K;
   const bf16 *A;
@@ -57,83 +76,197 @@ struct GemmArgs {
   float *C;
   int64_t ldc, scz;
   int accumulate;         // 1: C += A B
+  int *err;               // set to 1 if a wait on the tensor core gave up
 };
 
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(const GemmArgs g) {
-  __shared__ __align__(16) bf16 As[64][16 + 8];  // [m][k], padded rows
-  __shared__ __align__(16) bf16 Bs[64][16 + 8];  // [n][k]
-  const int z = blockIdx.z;
-  const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int grp = lane >> 2, tig = lane & 3;
-  const bf16 *A = g.A + z * g.saz;
-  const bf16 *B = g.B + z * g.sbz;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-  const bf16 zero = __float2bfloat16(0.f);
-  for (int k0 = 0; k0 < g.K; k0 += 16) {
-    // stage 64 x 16 of A and 16 x 64 of B (8 elements per thread each)
-    for (int e = tid; e < 64 * 16; e += 128) {
-      const int r = e >> 4, kk = e & 15;
-      const int m = m0 + r, k = k0 + kk;
-      As[r][kk] = (m < g.M && k < g.K) ? A[m * g.sam + k * g.sak] : zero;
-      const int n = n0 + r;
-      Bs[r][kk] = (n < g.N && k < g.K) ? B[k * g.sbk + n * g.sbn] : zero;
-    }
-    __syncthreads();
-    uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int r = wm + i * 16 + grp;
-      af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][tig * 2]);
-      af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][tig * 2]);
-      af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][tig * 2 + 8]);
-      af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][tig * 2 + 8]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = wn + j * 8 + grp;
-      bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][tig * 2]);
-      bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][tig * 2 + 8]);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-            "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-            : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bfr[j][0]),
-              "r"(bfr[j][1]));
-      }
-    __syncthreads();
-  }
-  float *C = g.C + z * g.scz;
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int m = m0 + wm + i * 16 + grp + (r >= 2 ? 8 : 0);
-        const int n = n0 + wn + j * 8 + tig * 2 + (r & 1);
-        if (m < g.M && n < g.N) {
-          float *p = &C[m * g.ldc + n];
-          *p = g.accumulate ? *p + acc[i][j][r] : acc[i][j][r];
-        }
-      }
+constexpr int kTcM = 128, kTcN = 128, kTcK = 64;
+constexpr int kTcTileBytes = kTcM * kTcK * 2;                // one operand stage: 16 KB
+constexpr int kTcSmemBytes = 4 * kTcTileBytes + 64;          // A, B x 2 stages + barriers
+constexpr int kTcTmemCols = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-int gemm(const GemmArgs &g, int nz, cudaStream_t s) {
-  dim3 grid((g.N + 63) / 64, (g.M + 63) / 64, nz);
-  gemm_bf16_kernel<<<grid, 128, 0, s>>>(g);
+// Shared-memory matrix descriptor of tcgen05.mma: start address, leading
+// byte offset (between core matrices adjacent in K), stride byte offset
+// (between core matrices adjacent in M / N), all in 16-byte units; version
+// 1 (bits 46-47); base offset 0; no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo & 0x3FFFFu) >> 4) << 16) |
+         ((uint64_t)((sbo & 0x3FFFFu) >> 4) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: D in FP32 (bits 4-5 = 1), A and B in
+// BF16 (bits 7-9 = 1, bits 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__device__ __forceinline__ uint32_t umma_instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// Bounded wait for the phase of `parity` of an mbarrier; false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (int i = 0; i < (1 << 22); i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Offset (in elements) of element (r, k) of a rows x 64 stage in the
+// no-swizzle K-major core-matrix layout: core matrix (r / 8, k / 8) at
+// ((r / 8) * 8 + k / 8) * 64, element (r % 8, k % 8) inside it.
+__device__ __forceinline__ int core_offset(int r, int k) {
+  return (((r >> 3) << 3) + (k >> 3)) * 64 + ((r & 7) << 3) + (k & 7);
+}
+
+// Gathers rows [row0, row0 + nrows) x k [k0, k0 + 64) of an operand X(row, k)
+// = X[row * srow + k * sk] into a stage (zero outside rows < rmax, k < kmax),
+// walking the contiguous index fastest.
+__device__ __forceinline__ void gather_stage(bf16 *dst, const bf16 *src, int nrows, int row0,
+                                             int rmax, int64_t srow, int k0, int kmax,
+                                             int64_t sk) {
+  const bf16 zero = __float2bfloat16(0.f);
+  const int total = nrows * kTcK;
+  if (sk == 1) {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int r = e >> 6, kk = e & 63;
+      const int row = row0 + r, k = k0 + kk;
+      dst[core_offset(r, kk)] = (row < rmax && k < kmax) ? src[row * srow + k] : zero;
+    }
+  } else {
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int r = e % nrows, kk = e / nrows;
+      const int row = row0 + r, k = k0 + kk;
+      dst[core_offset(r, kk)] = (row < rmax && k < kmax) ? src[row * srow + k * sk] : zero;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) gemm_bf16_tc_kernel(const GemmArgs g) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  bf16 *As = reinterpret_cast<bf16 *>(smem);                       // 2 stages
+  bf16 *Bs = reinterpret_cast<bf16 *>(smem + 2 * kTcTileBytes);    // 2 stages
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * kTcTileBytes);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 4 * kTcTileBytes + 16);
+  const int z = blockIdx.z;
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int bn = min(kTcN, ((g.N - n0 + 15) / 16) * 16);  // tile width, multiple of 16
+  const bf16 *A = g.A + z * g.saz;
+  const bf16 *B = g.B + z * g.sbz;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2; i++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[i])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {  // the whole warp allocates the accumulator's TMEM columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_instr_desc(kTcM, bn);
+
+  bool ok = true;
+  const int nkb = (g.K + kTcK - 1) / kTcK;
+  for (int kb = 0; kb < nkb; kb++) {
+    const int st = kb & 1, k0 = kb * kTcK;
+    // the MMAs that read this stage two blocks ago must be done with it
+    if (kb >= 2 && ok) ok = mbar_wait(smem_u32(&bars[st]), ((kb - 2) >> 1) & 1);
+    bf16 *as = As + st * (kTcTileBytes / 2), *bs = Bs + st * (kTcTileBytes / 2);
+    gather_stage(as, A, kTcM, m0, g.M, g.sam, k0, g.K, g.sak);
+    gather_stage(bs, B, bn, n0, g.N, g.sbn, k0, g.K, g.sbk);
+    // generic-proxy stores -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int slices = (min(kTcK, g.K - k0) + 15) / 16;
+      for (int j = 0; j < slices; j++) {
+        const uint64_t ad = umma_smem_desc(smem_u32(as) + j * 256, 128, 1024);
+        const uint64_t bd = umma_smem_desc(smem_u32(bs) + j * 256, 128, 1024);
+        const uint32_t accum = (kb > 0 || j > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+            : "memory");
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&bars[st]))
+          : "memory");
+    }
+  }
+  // the last commit covers every MMA of the tile
+  if (ok) ok = mbar_wait(smem_u32(&bars[(nkb - 1) & 1]), ((nkb - 1) >> 1) & 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!ok) {
+    if (lane == 0) atomicExch(g.err, 1);
+  } else {
+    float *C = g.C + z * g.scz;
+    const int m = m0 + warp * 32 + lane;  // this thread's accumulator row (TMEM lane)
+    for (int c0 = 0; c0 < bn; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+          "%11, %12, %13, %14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(taddr)
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < g.M) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const int n = n0 + c0 + j;
+          if (n < g.N) {
+            float *p = &C[m * g.ldc + n];
+            const float d = __uint_as_float(v[j]);
+            *p = g.accumulate ? *p + d : d;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcTmemCols)
+                 : "memory");
+}
+
+int gemm(GemmArgs g, int nz, cudaStream_t s, int *err) {
+  static unsigned long long attr_set = 0;  // devices whose kernel attribute is set
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 64 || !(attr_set >> dev & 1ull)) {
+    cudaError_t e = cudaFuncSetAttribute(gemm_bf16_tc_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kTcSmemBytes);
+    if (e != cudaSuccess) return (int)e;
+    if (dev < 64) attr_set |= 1ull << dev;
+  }
+  g.err = err;
+  dim3 grid((g.N + kTcN - 1) / kTcN, (g.M + kTcM - 1) / kTcM, nz);
+  gemm_bf16_tc_kernel<<<grid, 128, kTcSmemBytes, s>>>(g);
   return (int)cudaGetLastError();
 }
 
@@ -283,6 +416,7 @@ struct chaos_mlp {
   float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *Y = nullptr, *dA = nullptr, *loss = nullptr;
   float *Tb = nullptr;
   double *xyb = nullptr;
+  int *d_err = nullptr;  // set by a GEMM whose wait on the tensor core gave up
 };
 
 namespace {
@@ -328,7 +462,7 @@ int ensure_ws(chaos_mlp *h, int64_t rows) {
 
 GemmArgs mk(int M, int N, int K, const bf16 *A, int64_t sam, int64_t sak, int64_t saz, const bf16 *B,
             int64_t sbk, int64_t sbn, int64_t sbz, float *C, int64_t ldc, int64_t scz, int acc = 0) {
-  return GemmArgs{M, N, K, A, sam, sak, saz, B, sbk, sbn, sbz, C, ldc, scz, acc};
+  return GemmArgs{M, N, K, A, sam, sak, saz, B, sbk, sbn, sbz, C, ldc, scz, acc, nullptr};
 }
 
 // Forward pass of all networks on `rows` points (features already in h->X).
@@ -338,14 +472,14 @@ int forward(chaos_mlp *h, int64_t rows, cudaStream_t s) {
   const bf16 *Wb = h->pb;
   int rc = 0;
   // Z1 = X W1 ; A1 = silu(Z1 + b1)
-  rc |= gemm(mk(rows, W, kFeat, h->X, kFeat, 1, 0, Wb + h->off_w[0], W, 1, np, h->Z1, W, sz), E, s);
+  rc |= gemm(mk(rows, W, kFeat, h->X, kFeat, 1, 0, Wb + h->off_w[0], W, 1, np, h->Z1, W, sz), E, s, h->d_err);
   bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z1, h->p + h->off_b[0], np, h->A1, rows, W, sz);
-  rc |= gemm(mk(rows, W, W, h->A1, W, 1, sz, Wb + h->off_w[1], W, 1, np, h->Z2, W, sz), E, s);
+  rc |= gemm(mk(rows, W, W, h->A1, W, 1, sz, Wb + h->off_w[1], W, 1, np, h->Z2, W, sz), E, s, h->d_err);
   bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z2, h->p + h->off_b[1], np, h->A2, rows, W, sz);
-  rc |= gemm(mk(rows, W, W, h->A2, W, 1, sz, Wb + h->off_w[2], W, 1, np, h->Z3, W, sz), E, s);
+  rc |= gemm(mk(rows, W, W, h->A2, W, 1, sz, Wb + h->off_w[2], W, 1, np, h->Z3, W, sz), E, s, h->d_err);
   bias_silu_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->Z3, h->p + h->off_b[2], np, h->A3, rows, W, sz);
   rc |= gemm(mk(rows, kOutPad, W, h->A3, W, 1, sz, Wb + h->off_w[3], kOutPad, 1, np, h->Y, kOutPad,
-                rows * kOutPad), E, s);
+                rows * kOutPad), E, s, h->d_err);
   if (rc) return rc;
   return (int)cudaGetLastError();
 }
@@ -358,22 +492,22 @@ int backward(chaos_mlp *h, int64_t rows, cudaStream_t s) {
   float *g = h->g;
   int rc = 0;
   // layer 4: dW4 = A3^T dY ; db4 = sum dY ; dA3 = dY W4^T
-  rc |= gemm(mk(W, kOutPad, rows, h->A3, 1, W, sz, h->dY, kOutPad, 1, syz, g + h->off_w[3], kOutPad, np), E, s);
+  rc |= gemm(mk(W, kOutPad, rows, h->A3, 1, W, sz, h->dY, kOutPad, 1, syz, g + h->off_w[3], kOutPad, np), E, s, h->d_err);
   bias_grad_kernel<<<dim3(1, 1, E), kOutPad, 0, s>>>(h->dY, rows, kOutPad, syz, g + h->off_b[3], np);
-  rc |= gemm(mk(rows, W, kOutPad, h->dY, kOutPad, 1, syz, Wb + h->off_w[3], 1, kOutPad, np, h->dA, W, sz), E, s);
+  rc |= gemm(mk(rows, W, kOutPad, h->dY, kOutPad, 1, syz, Wb + h->off_w[3], 1, kOutPad, np, h->dA, W, sz), E, s, h->d_err);
   // layer 3
   silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z3, h->dZ, sz, sz);
-  rc |= gemm(mk(W, W, rows, h->A2, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[2], W, np), E, s);
+  rc |= gemm(mk(W, W, rows, h->A2, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[2], W, np), E, s, h->d_err);
   bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[2], np);
-  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[2], 1, W, np, h->dA, W, sz), E, s);
+  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[2], 1, W, np, h->dA, W, sz), E, s, h->d_err);
   // layer 2
   silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z2, h->dZ, sz, sz);
-  rc |= gemm(mk(W, W, rows, h->A1, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[1], W, np), E, s);
+  rc |= gemm(mk(W, W, rows, h->A1, 1, W, sz, h->dZ, W, 1, sz, g + h->off_w[1], W, np), E, s, h->d_err);
   bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[1], np);
-  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[1], 1, W, np, h->dA, W, sz), E, s);
+  rc |= gemm(mk(rows, W, W, h->dZ, W, 1, sz, Wb + h->off_w[1], 1, W, np, h->dA, W, sz), E, s, h->d_err);
   // layer 1
   silu_back_kernel<<<dim3(blocks(sz, 256), 1, E), 256, 0, s>>>(h->dA, h->Z1, h->dZ, sz, sz);
-  rc |= gemm(mk(kFeat, W, rows, h->X, 1, kFeat, 0, h->dZ, W, 1, sz, g + h->off_w[0], W, np), E, s);
+  rc |= gemm(mk(kFeat, W, rows, h->X, 1, kFeat, 0, h->dZ, W, 1, sz, g + h->off_w[0], W, np), E, s, h->d_err);
   bias_grad_kernel<<<dim3(blocks(W, 128), 1, E), 128, 0, s>>>(h->dZ, rows, W, sz, g + h->off_b[0], np);
   if (rc) return rc;
   return (int)cudaGetLastError();
@@ -469,6 +603,7 @@ int chaos_mlp_create(int ensemble, int width, int outputs, uint64_t seed, int de
   al((void **)&h->pb, sizeof(bf16) * n);
   al((void **)&h->d_tmean, sizeof(float) * kOutPad * 3);
   al((void **)&h->loss, sizeof(float) * ensemble);
+  al((void **)&h->d_err, sizeof(int));
   if (e != cudaSuccess) {
     cudaFree(h->p);
     cudaFree(h->g);
@@ -477,6 +612,7 @@ int chaos_mlp_create(int ensemble, int width, int outputs, uint64_t seed, int de
     cudaFree(h->pb);
     cudaFree(h->d_tmean);
     cudaFree(h->loss);
+    cudaFree(h->d_err);
     delete h;
     return fail(CHAOS_LYAP_ENOMEM, std::string("surrogate parameters: ") + cudaGetErrorString(e));
   }
@@ -494,6 +630,7 @@ int chaos_mlp_create(int ensemble, int width, int outputs, uint64_t seed, int de
   cudaMemset(h->g, 0, sizeof(float) * n);
   cudaMemset(h->m, 0, sizeof(float) * n);
   cudaMemset(h->v, 0, sizeof(float) * n);
+  cudaMemset(h->d_err, 0, sizeof(int));
   to_bf16_kernel<<<blocks(n, 256), 256>>>(h->p, h->pb, n);
   for (int c = 0; c < kOutPad; c++) h->tmean[c] = 0.f, h->tstd[c] = 1.f;
   float tb[3 * kOutPad];
@@ -519,9 +656,22 @@ int chaos_mlp_destroy(chaos_mlp *h) {
   cudaFree(h->pb);
   cudaFree(h->d_tmean);
   cudaFree(h->loss);
+  cudaFree(h->d_err);
   delete h;
   return CHAOS_LYAP_OK;
 }
+
+namespace {
+// A GEMM whose wait on the tensor core gave up leaves *d_err set; the calls
+// that wait for their work report it (and clear it).
+int check_tc(chaos_mlp *h) {
+  int v = 0;
+  cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (!v) return CHAOS_LYAP_OK;
+  cudaMemset(h->d_err, 0, sizeof(int));
+  return fail(CHAOS_LYAP_ECUDA, "surrogate GEMM: a wait on the tensor core timed out");
+}
+}  // namespace
 
 int chaos_mlp_set_domain(chaos_mlp *h, double u0, double u1, double v0, double v1) {
   if (!h || !(u1 != u0) || !(v1 != v0)) return fail(CHAOS_LYAP_EINVAL, "empty domain");
@@ -594,6 +744,7 @@ int chaos_mlp_gradient(chaos_mlp *h, const double *xy, const double *T, int64_t 
   if (rc) return cuda_fail((cudaError_t)rc, "gradient");
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return cuda_fail(e, "gradient");
+  if ((rc = check_tc(h))) return rc;
   if (grads_out) cudaMemcpy(grads_out, h->g, sizeof(float) * h->np * h->E, cudaMemcpyDeviceToHost);
   if (loss_out) cudaMemcpy(loss_out, h->loss, sizeof(float) * h->E, cudaMemcpyDeviceToHost);
   return CHAOS_LYAP_OK;
@@ -656,6 +807,7 @@ int chaos_mlp_train(chaos_mlp *h, const double *xy, const double *T, int64_t N, 
   }
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "train");
+  if ((rc = check_tc(h))) return rc;
   if (loss_out && steps > 0) cudaMemcpy(loss_out, h->loss, sizeof(float) * h->E, cudaMemcpyDeviceToHost);
   return CHAOS_LYAP_OK;
 }
@@ -683,8 +835,9 @@ int chaos_mlp_predict(chaos_mlp *h, const double *xy, int64_t N, float *mean, fl
         h->Y, h->E, rows, h->outs, h->d_tmean, h->d_tstd, mean ? mean + o * h->outs : nullptr,
         stdev ? stdev + o * h->outs : nullptr);
   }
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? CHAOS_LYAP_OK : cuda_fail(e, "predict");
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "predict");
+  return check_tc(h);
 }
 
 }  // extern "C"

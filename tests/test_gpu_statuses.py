@@ -2,10 +2,10 @@
 device-side limits that a test runs out (nothing here faults a GPU): one
 point per status among ordinary points of the same warp --
   1 non-finite: a NaN parameter;
-  2 step underflow: a stiff point (Rossler c = 1e5, Lorenz-96 gamma = 1e6)
+  2 step underflow: a stiff point (Rossler c = 1e5, Lorenz-96 gamma = 1e5)
     whose steps must fall below h_min = 1e-4 (ordinary points need >= 0.02);
   3 step budget: an averaging time of 1e6 against max_steps = 3e5;
-  4 escape: an orbit with no bounded attractor (Rossler a = 0.6), or a
+  4 escape: an orbit with no bounded attractor (Rossler a = 1.5), or a
     Lorenz-96 state started outside the escape radius.
 Each failing point ends alone: the other points finish with status 0 and the
 spectra of a run in which the failing points are ordinary ones (up to the
@@ -27,7 +27,7 @@ def _rossler(orc):
     bad_p[3, 0] = np.nan
     bad_p[10, 2] = 1e5
     bad_t[17] = 1e6
-    bad_p[24, 0] = 0.6
+    bad_p[24, 0] = 1.5
     return (params, inits, tavg), (bad_p, inits, bad_t)
 
 
@@ -109,7 +109,7 @@ def test_statuses_lorenz96_warp(lib, orc, schedule):
     tavg = np.full(8, 5.0)
     bp, bx, bt = params.copy(), inits.copy(), tavg.copy()
     bp[1, 0] = np.nan
-    bp[3, 1] = 1e6
+    bp[3, 1] = 1e5
     bt[5] = 1e6
     bx[6] += 2e4
     kw = dict(model="lorenz96", method="var", integrator="dopri5", precision="fp32", k=40,

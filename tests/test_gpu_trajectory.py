@@ -3,7 +3,10 @@
 against trajectories of the reference's own dopriStep
 (tests/golden/reference_dopri.npz): FP64 follows the reference's step
 sequence within rounding; the bounds and why they are not zero are in
-trajectory_cases.py."""
+trajectory_cases.py.  (The FP32 form is not held to the reference's step
+sequence: in FP32 the error estimate's rounding noise at rtol 1e-6 is a
+sizeable part of the estimate itself, so its steps legitimately differ; its
+accuracy is tested on the spectra.)"""
 import numpy as np
 import pytest
 
@@ -32,18 +35,6 @@ def test_fp64_trajectory_follows_reference_dopri(lib, name):
     for i in range(3):  # every lane of the launch computes the same sequence
         assert np.array_equal(t[i], t[0]) and np.array_equal(x[i], x[0])
     tc.assert_follows_reference(t[0], h[0], x[0], c)
-
-
-@pytest.mark.parametrize("name", ["lorenz_6", "rossler_6", "shimizu_6"])
-def test_fp32_trajectory_tracks_reference_dopri(lib, name):
-    """The FP32 form (state in FP32, controller in FP32 with fast
-    reciprocals) follows the same step law: over its first 50 steps the times
-    stay within FP32 rounding of the reference's."""
-    c = tc.case(name)
-    t, h, x, st = _trajectory(lib, c, "fp32")
-    assert st[0] == 0
-    np.testing.assert_allclose(t[0, :50], c["t"][:50], rtol=1e-4)
-    np.testing.assert_allclose(h[0, :50], c["h"][:50], rtol=1e-3)
 
 
 def test_trajectory_statuses(lib):
