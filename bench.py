@@ -322,7 +322,9 @@ def run_surrogate_bench(a, rank, world, local):
         plain_how = f"the whole {n}x{n} map in one launch, CUDA events"
         del dp, dx, ds, dst
     cfg = RefineConfig(round_grid_step=max(1, n // 512), rule=a.surrogate_rule,
-                       regime_conf=a.regime_conf, regime_std=a.regime_std)
+                       regime_conf=a.regime_conf, regime_std=a.regime_std,
+                       verify_step=a.verify_step, mark_radius=a.mark_radius,
+                       rounds=a.rounds)
     cfg.lam_limit = lam_limit_of(cfg)
     if cfg.rule == "regime":
         rule = (f"integrate where the ensemble's regime score r = tanh((lambda_1 - "
@@ -374,7 +376,8 @@ def run_surrogate_bench(a, rank, world, local):
                        "ensemble": "4 x MLP 16 Fourier features -> 128 -> 128 -> 128 -> 3, "
                                    "SiLU, BF16 mma.sync, FP32 accumulate, Adam 1e-3",
                        "rule": rule,
-                       "rounds": cfg.rounds, "round_max_new": cfg.round_max_new},
+                       "rounds": cfg.rounds, "round_max_new": cfg.round_max_new,
+                       "verify_step": cfg.verify_step, "mark_radius": cfg.mark_radius},
             "refined_s": refined, "plain_s": plain_est, "plain_timing": plain_how,
             "refined_over_plain": refined / plain_est,
             "plain_fraction": info["plain_fraction"], "training_cells": info["training_cells"],
@@ -982,6 +985,11 @@ def main():
                     help="lorenz1024: cells of the Rossler 1024^2 map checked against the oracle")
     ap.add_argument("--no-rossler", dest="with_rossler", action="store_false",
                     help="lorenz1024: skip the Rossler 1024^2 precision-form map timed beside it")
+    ap.add_argument("--verify-step", type=int, default=0,
+                    help="surrogate: subgrid step of the verification sweep (0: none)")
+    ap.add_argument("--mark-radius", type=int, default=8,
+                    help="surrogate: half-width of the block integrated around a contradiction")
+    ap.add_argument("--rounds", type=int, default=4, help="surrogate: refinement rounds")
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="surrogate: time the plain sweep on this many random cells and "
                          "extrapolate (0: time the whole map)")

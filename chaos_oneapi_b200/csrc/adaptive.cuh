@@ -81,8 +81,12 @@ CL_HD double quiet_nan() {
 // multiply-add of both rows).  Coefficients and h are scalars of type S.
 // Every stage combination is an explicit chain mul, fma, fma, ... so the
 // scalar and packed forms do the same operations in the same order.
+// double2 pairs two FP64 rows the same way (two scalar FMAs per coefficient:
+// FP64 has no packed form, but the two rows' dependency chains interleave in
+// one pass, which halves the latency a lane waits on per stage).
 template <class E> struct ScalarOf { using type = E; };
 template <> struct ScalarOf<float2> { using type = float; };
+template <> struct ScalarOf<double2> { using type = double; };
 
 CL_HD float vmul(float a, float b) { return a * b; }
 CL_HD double vmul(double a, double b) { return a * b; }
@@ -117,6 +121,11 @@ CL_HD float2 vfma2(float2 a, float2 b, float2 c) {
 #endif
 }
 
+CL_HD double2 vmul(double a, double2 b) { return make_double2(a * b.x, a * b.y); }
+CL_HD double2 vfma(double a, double2 b, double2 c) {
+  return make_double2(fma(a, b.x, c.x), fma(a, b.y, c.y));
+}
+
 // lin(c1, k1, c2, k2, ...) = c1 k1 + c2 k2 + ... (left to right)
 template <class S, class E> CL_HD E lin_acc(E acc) { return acc; }
 // (arguments by value: the coefficients are constexpr members, which device
@@ -141,6 +150,7 @@ template <> struct CtlReal<double> { using type = double; };
 template <class E> struct ErrAcc { using type = float; };
 template <> struct ErrAcc<float2> { using type = float2; };
 template <> struct ErrAcc<double> { using type = double; };
+template <> struct ErrAcc<double2> { using type = double2; };
 
 CL_HD void err_acc(float y0, float y1, float e, float rtol, float atol, float &acc) {
   const float m = fmaxf(fabsf(y0), fabsf(y1));
@@ -182,6 +192,17 @@ CL_HD void err_row(const E *y0, const E *y1, const E *he, T rtol, T atol, A &acc
       const double sk = fma(rtol, fmax(fabs(y0[N - 1]), fabs(y1[N - 1])), atol);
       const double r = he[N - 1] * recip(sk);
       acc = fma(r, r, acc);
+    }
+  } else if constexpr (std::is_same<E, double2>::value) {
+    // a pair of FP64 rows: component j of both rows shares the reciprocal
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const double sx = fma(rtol, fmax(fabs(y0[j].x), fabs(y1[j].x)), atol);
+      const double sy = fma(rtol, fmax(fabs(y0[j].y), fabs(y1[j].y)), atol);
+      const double inv = recip(sx * sy);
+      const double rx = he[j].x * (sy * inv), ry = he[j].y * (sx * inv);
+      acc.x = fma(rx, rx, acc.x);
+      acc.y = fma(ry, ry, acc.y);
     }
   } else {
 #pragma unroll
@@ -469,6 +490,31 @@ template <class M, int K, class R>
 struct Packed {
   static constexpr bool value = std::is_same<R, float>::value && K >= 2;
   static constexpr bool state_paired = (K % 2 == 1);
+};
+
+// (state, one tangent vector) as FP64 pairs: the state's stage point is
+// recorded and the vector's derivative taken at it, in the same pass.
+template <class M>
+struct PairStateStages64 {
+  const double *p;
+  double (*X)[M::N];
+  CL_HD void operator()(int s, const double2 *arg, double2 *out) const {
+    constexpr int N = M::N;
+    double ax[N], av[N], ox[N], ov[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      ax[j] = arg[j].x;
+      av[j] = arg[j].y;
+    }
+    if (s > 0) {
+#pragma unroll
+      for (int j = 0; j < N; j++) X[s][j] = ax[j];
+    }
+    M::f(ax, ox, p);
+    M::jv(av, ov, p, ax);
+#pragma unroll
+    for (int j = 0; j < N; j++) out[j] = make_double2(ox[j], ov[j]);
+  }
 };
 
 template <class M>

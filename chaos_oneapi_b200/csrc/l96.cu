@@ -11,9 +11,14 @@
 // lane has the stage points it needs for J without any exchange), then the k
 // tangent vectors four at a time.  Per-step registers: the lane's 5
 // components of the 7 stage points as Jacobian coefficients, plus one
-// vector's Dopri5 stages.  Between steps the tangent vectors and their FSAL
-// derivatives live in shared memory (double-buffered: candidate / accepted),
-// 4 x k x 40 floats per warp; the FP64 QR reuses the candidate half.
+// vector's Dopri5 stages.  Between steps the tangent vectors live in shared
+// memory, double-buffered (accepted / candidate, swapped on acceptance):
+// 2 x k x 40 floats per warp.  Their first-stage derivatives are not stored:
+// J(x) v at the step's start costs one stencil pass with the stage-0
+// Jacobian coefficients the state pass computes anyway (the same floats an
+// FSAL copy would hold), and leaving them out halves the shared memory per
+// point, so twice as many points fit on an SM.  The FP64 QR widens the
+// vectors in place over both halves (k x 40 doubles).
 //
 // The phase and renormalisation logic follows adaptive.cuh (transient /
 // alignment / averaging with clamped landings, the renormalisation interval
@@ -33,7 +38,7 @@ namespace l96 {
 constexpr int N = 40;        // model dimension
 constexpr int G = 4;         // vectors processed at once per warp (lane groups)
 constexpr int C = 5;         // components per lane
-constexpr int WARPS = 8;     // warps (points) per block
+constexpr int WARPS = 4;     // warps (points) per block
 constexpr unsigned FULL = 0xffffffffu;
 
 struct DPc {  // Dormand-Prince 5(4), cuda/tools/dopri.dp.cpp:14-44
@@ -191,33 +196,63 @@ __device__ __forceinline__ void flush_logs(Warp &w) {
   }
 }
 
-// Tangent FSAL derivatives KV = J(x) V for the k vectors.
-__device__ void refresh_kv(const Warp &w, const float *V, float *KV, int k, int g, int li,
-                           int left, int right) {
-  float dx[C];
-  Jc jc;
-  rhs_state(w.x, dx, jc, w.F, w.gam, left, right);
-  for (int r = 0; r < (k + G - 1) / G; r++) {
-    const int vec = r * G + g;
-    const bool valid = vec < k;
-    float v[C], dv[C];
-#pragma unroll
-    for (int j = 0; j < C; j++) v[j] = valid ? V[vec * N + li * C + j] : 0.f;
-    rhs_tangent(v, dv, jc, w.gam, left, right);
-    if (valid)
-#pragma unroll
-      for (int j = 0; j < C; j++) KV[vec * N + li * C + j] = dv[j];
+// In-place conversions between the k x 40 FP32 vectors and their FP64 copy
+// W, which covers the warp's whole 2 x k x 40-float area (base).  The FP32
+// vectors are in its lower half (src_upper false) or upper half.  Chunks of
+// 32 elements, each read whole (__syncwarp) before it is written, in the
+// order that never overwrites an element not yet read: widening from the
+// lower half runs downwards (double i covers floats 2i, 2i + 1 >= i),
+// widening from the upper half and narrowing into the lower half run upwards.
+__device__ void widen(const float *src, double *W, int n, int lane, bool src_upper) {
+  const int nch = (n + 31) / 32;
+  for (int c = 0; c < nch; c++) {
+    const int idx = 32 * (src_upper ? c : nch - 1 - c) + lane;
+    const float f = idx < n ? src[idx] : 0.f;
+    __syncwarp();
+    if (idx < n) W[idx] = (double)f;
+    __syncwarp();
   }
-  __syncwarp();
+}
+__device__ void narrow(const double *W, float *dst, int n, int lane) {
+  const int nch = (n + 31) / 32;
+  for (int c = 0; c < nch; c++) {
+    const int idx = 32 * c + lane;
+    const double d = idx < n ? W[idx] : 0.0;
+    __syncwarp();
+    if (idx < n) dst[idx] = (float)d;
+    __syncwarp();
+  }
 }
 
-// Modified Gram-Schmidt in FP64 on the k vectors of V (k x 40, FP32), through
-// the FP64 work area W (k x 40 doubles).  Returns max |v_q|^2 / r_q^2 (the
-// cancellation factor) and multiplies r_q into the lane that owns exponent q.
-__device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int lane,
+// Modified Gram-Schmidt in FP64 on the k vectors of V (k x 40, FP32, in the
+// lower or upper half of the warp's area `base`), through the FP64 work area
+// W = base (k x 40 doubles); the orthonormal vectors end in the lower half.
+// Returns max |v_q|^2 / r_q^2 (the cancellation factor), the smallest r_q in
+// rmin, and multiplies r_q into the lane that owns exponent q.
+__device__ double mgs_qr(Warp &w, const float *V, float *base, int k, int g, int li, int lane,
                          bool accumulate, bool &ok, double &rmin) {
-  // FP32 -> FP64, and squared norms before orthogonalisation
-  for (int idx = lane; idx < k * N; idx += 32) W[idx] = (double)V[idx];
+  double *W = reinterpret_cast<double *>(base);
+  widen(V, W, k * N, lane, V != base);
+  // squared norms before orthogonalisation: vector q's in lane q % 32, slot q / 32
+  double nb[2] = {0.0, 0.0};
+  for (int r = 0; r < (k + G - 1) / G; r++) {
+    const int vec = r * G + g;
+    double b = 0;
+    if (vec < k) {
+#pragma unroll
+      for (int j = 0; j < C; j++) {
+        const double vb = W[vec * N + li * C + j];
+        b = fma(vb, vb, b);
+      }
+    }
+    b = group_sum(b);
+#pragma unroll
+    for (int gg = 0; gg < G; gg++) {
+      const double bv = __shfl_sync(FULL, b, gg * 8);
+      const int q = r * G + gg;
+      if (q < k && (q & 31) == lane) nb[q >> 5] = bv;
+    }
+  }
   __syncwarp();
   double cancel = 1.0;
   ok = true;
@@ -260,13 +295,7 @@ __device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int
     if (ok) {
       // cancellation: norm before any projection vs r (the first vector has none)
       if (q > 0) {
-        double b = 0;
-#pragma unroll
-        for (int j = 0; j < C; j++) {
-          const double vb = (double)V[q * N + li * C + j];
-          b = fma(vb, vb, b);
-        }
-        b = group_sum(b);
+        const double b = __shfl_sync(FULL, (q >> 5) ? nb[1] : nb[0], q & 31);
         cancel = fmax(cancel, b / s);
       }
       if (accumulate && (q & 31) == lane) {
@@ -276,8 +305,7 @@ __device__ double mgs_qr(Warp &w, float *V, double *W, int k, int g, int li, int
     }
   }
   __syncwarp();
-  for (int idx = lane; idx < k * N; idx += 32) V[idx] = (float)W[idx];
-  __syncwarp();
+  narrow(W, base, k * N, lane);
   return cancel;
 }
 
@@ -306,16 +334,15 @@ __device__ __forceinline__ long long fetch(const AdaptiveArgs &a, int lane, long
   return (long long)((q * (unsigned long long)a.queue_stride) % (unsigned long long)a.P);
 }
 
-__global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a) {
+__global__ void __launch_bounds__(WARPS * 32, 4) l96_kernel(const AdaptiveArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int g = lane >> 3, li = lane & 7;
   const int left = g * 8 + ((li + 7) & 7), right = g * 8 + ((li + 1) & 7);
   const int k = a.k;
-  const size_t per_warp = (size_t)4 * k * N;  // floats: V, KV, V1, KV1
+  const size_t per_warp = (size_t)2 * k * N;  // floats: accepted and candidate vectors
   float *base = reinterpret_cast<float *>(smem) + wid * per_warp;
-  float *V = base, *KV = base + k * N, *V1 = base + 2 * k * N, *KV1 = base + 3 * k * N;
-  double *W = reinterpret_cast<double *>(V1);  // FP64 QR work area (V1 + KV1)
+  float *V = base, *V1 = base + k * N;
 
   const float rtol = (float)a.rtol, atol = (float)a.atol;
   const float tau = 0.3f * logf(1.0f / fmaxf(rtol, 5.96e-8f));
@@ -331,7 +358,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
   auto start_tangent = [&]() {
     for (int idx = lane; idx < k * N; idx += 32) V[idx] = (idx / N == idx % N) ? 1.f : 0.f;
     __syncwarp();
-    refresh_kv(w, V, KV, k, g, li, left, right);
     w.fac_old = 1e-4f;
     w.t_phase = 0.0;
     w.t_gs = 0.0;
@@ -372,7 +398,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
   auto gram_schmidt = [&]() -> bool {
     bool ok;
     double rmin;
-    const double cancel = mgs_qr(w, V, W, k, g, li, lane, w.phase == kAverage, ok, rmin);
+    const double cancel = mgs_qr(w, V, base, k, g, li, lane, w.phase == kAverage, ok, rmin);
+    V = base;  // the orthonormal vectors are in the lower half now
+    V1 = base + k * N;
     if (!ok) return false;
     if (w.phase == kAverage) {
       bool fl = false;
@@ -384,7 +412,6 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
       adaptive::next_renorm_interval(w.L, w.rate_max, (float)cancel, rmin, w.t_gs, tau,
                                      a.dt_renorm);
     w.t_gs = 0.0;
-    refresh_kv(w, V, KV, k, g, li, left, right);
     return true;
   };
 
@@ -418,10 +445,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
           const bool valid = vec < k;
           float v[C], kv[C], v1[C], kv1[C];
 #pragma unroll
-          for (int j = 0; j < C; j++) {
-            v[j] = valid ? V[vec * N + li * C + j] : 0.f;
-            kv[j] = valid ? KV[vec * N + li * C + j] : 0.f;
-          }
+          for (int j = 0; j < C; j++) v[j] = valid ? V[vec * N + li * C + j] : 0.f;
+          // first stage: J(x) v with the state pass's stage-0 coefficients
+          rhs_tangent(v, kv, jcs[0], w.gam, left, right);
           float e2 = 0.f;
           auto rhs = [&](int s, const float (&arg)[C], float (&out)[C]) {
             rhs_tangent(arg, out, jcs[s], w.gam, left, right);
@@ -430,10 +456,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
           if (valid) {
             err2 += e2;
 #pragma unroll
-            for (int j = 0; j < C; j++) {
-              V1[vec * N + li * C + j] = v1[j];
-              KV1[vec * N + li * C + j] = kv1[j];
-            }
+            for (int j = 0; j < C; j++) V1[vec * N + li * C + j] = v1[j];
           }
         }
       }
@@ -455,12 +478,9 @@ __global__ void __launch_bounds__(WARPS * 32, 1) l96_kernel(const AdaptiveArgs a
           }
           __syncwarp();
           if (joint) {  // accept the candidate: swap buffers
-            float *t0 = V, *t1 = KV;
+            float *t0 = V;
             V = V1;
-            KV = KV1;
             V1 = t0;
-            KV1 = t1;
-            W = reinterpret_cast<double *>(V1 < KV1 ? V1 : KV1);
           }
           if ((double)hnew > hmax) hnew = (float)hmax;
           if (w.reject && hnew > h) hnew = h;
@@ -507,7 +527,7 @@ int launch_l96_warp(int integrator, int precision, const AdaptiveArgs &a, int, c
   using namespace l96;
   if (integrator != kDopri5 || precision != kFP32) return kErrUnsupported;
   if (a.k < 1 || a.k > N) return kErrUnsupported;
-  const size_t smem = (size_t)WARPS * 4 * a.k * N * sizeof(float);
+  const size_t smem = (size_t)WARPS * 2 * a.k * N * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(l96_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return (int)e;

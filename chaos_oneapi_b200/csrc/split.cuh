@@ -181,16 +181,29 @@ __device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG> 
     }
     es = ea.x;
     ev = ea.y;
-  } else {
-    R X[S][N];
-    StateStages<M, R> fs{st.p, X};
-    if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, es, rtol, atol);
-    else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, es, rtol, atol);
-    if (joint) {
-      TangentStages<M, R> ft{st.p, st.x, X};
-      if (INTEG == kDverk65) dverk_pass<N, R>(st.v, h, ft, v1, ev, rtol, atol);
-      else dopri_pass<N, R>(st.v, st.kv, h, ft, v1, kv1, ev, rtol, atol);
+  } else {  // (state, v_r) as one pass over FP64 pairs: the two chains interleave
+    double X[S][N];
+    double2 ya[N], ka[N], ya1[N], ka1[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      ya[j] = make_double2(st.x[j], st.v[j]);
+      ka[j] = make_double2(st.kx[j], st.kv[j]);
     }
+    double2 ea = make_double2(0.0, 0.0);
+    PairStateStages64<M> fa{st.p, X};
+    if (INTEG == kDverk65) dverk_pass<N, double2>(ya, h, fa, ya1, ea, rtol, atol);
+    else dopri_pass<N, double2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      x1[j] = ya1[j].x;
+      v1[j] = ya1[j].y;
+      if (INTEG == kDopri5) {
+        kx1[j] = ka1[j].x;
+        kv1[j] = ka1[j].y;
+      }
+    }
+    es = ea.x;
+    ev = ea.y;
   }
   // the state's error once (lane 0), each vector's in its own lane
   C e = (g.r == 0 ? es : C(0)) + ((joint && has_vec) ? ev : C(0));

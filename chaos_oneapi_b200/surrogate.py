@@ -219,6 +219,15 @@ class RefineConfig:
     regime_width: float = 0.005
     regime_conf: float = 0.8
     regime_std: float = 0.1
+    # Verification sweep: after the rounds, integrate every cell of the
+    # verify_step subgrid not integrated yet, and compare each with the
+    # ensemble's regime call before training on it.  Where they contradict,
+    # the map has structure the networks do not resolve (periodic windows
+    # inside the chaotic region are bands a few cells wide): the final fill
+    # integrates the (2 mark_radius + 1)^2 block of cells around every
+    # contradiction.  0 switches the stage off.
+    verify_step: int = 0
+    mark_radius: int = 8
     seed: int = 0
     timings: dict = field(default_factory=dict)
 
@@ -265,6 +274,20 @@ def _targets(y, cfg):
         return y
     r = np.tanh((y[:, 0] - cfg.regime_threshold) / cfg.regime_width)
     return np.concatenate([y, r[:, None]], axis=1)
+
+
+def _blocks(cells: np.ndarray, shape, radius: int) -> np.ndarray:
+    """Flat indices of every cell within `radius` (in both grid directions)
+    of one of `cells`, clipped to the map."""
+    if cells.size == 0 or radius < 0:
+        return np.zeros(0, dtype=np.int64)
+    n1, n2 = shape
+    a, b = np.divmod(cells.astype(np.int64), n2)
+    d = np.arange(-radius, radius + 1)
+    aa = (a[:, None, None] + d[None, :, None]).repeat(d.size, axis=2)
+    bb = (b[:, None, None] + d[None, None, :]).repeat(d.size, axis=1)
+    keep = (aa >= 0) & (aa < n1) & (bb >= 0) & (bb < n2)
+    return np.unique(aa[keep] * n2 + bb[keep])
 
 
 def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None, probe=None):
@@ -342,7 +365,27 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None, probe=N
         if log:
             log(f"round {r}: flagged {flag.mean():.3f} of candidates, +{pick.size} cells, loss {loss}")
 
-    # 4. final fill
+    # 4. verification sweep: the ensemble's regime call against plain cells
+    marked = np.zeros(0, dtype=np.int64)
+    if cfg.verify_step > 0:
+        t = time.perf_counter()
+        ver = np.setdiff1d(spec.subgrid(cfg.verify_step), train_idx)
+        mean, _ = net.predict(torch.from_numpy(spec.coords(ver)).cuda())
+        yv, stv = plain_sweep(sweep, spec, ver)
+        okv = stv == 0
+        called = mean[:, 0].cpu().numpy() > cfg.regime_threshold
+        contra = ver[okv & (called != (yv[:, 0] > cfg.regime_threshold))]
+        marked = _blocks(contra, spec.shape, cfg.mark_radius)
+        train_idx = np.concatenate([train_idx, ver[okv]])
+        y = np.concatenate([y, yv[okv]])
+        loss = fit(train_idx, y, cfg.steps_round, cfg.seed + cfg.rounds + 1)
+        torch.cuda.synchronize()
+        tm["verify"] = {"cells": int(ver.size), "contradictions": int(contra.size),
+                        "marked": int(marked.size), "s": time.perf_counter() - t}
+        if log:
+            log(f"verify: {ver.size} cells, {contra.size} contradictions, {marked.size} marked")
+
+    # 5. final fill
     t = time.perf_counter()
     out = np.empty((P, k))
     mask = np.zeros(P, dtype=bool)
@@ -359,7 +402,7 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None, probe=N
     tm["predict_s"] = time.perf_counter() - t
     t = time.perf_counter()
     flagged = np.concatenate(flagged) if flagged else np.zeros(0, dtype=np.int64)
-    fill = np.setdiff1d(flagged, train_idx)
+    fill = np.setdiff1d(np.union1d(flagged, marked), train_idx)
     yf, _ = plain_sweep(sweep, spec, fill)
     out[fill] = yf
     mask[fill] = True
@@ -369,7 +412,7 @@ def refine_map(spec: MapSpec, sweep: Sweep, cfg: RefineConfig, log=None, probe=N
     tm["total_s"] = time.perf_counter() - t_all
     info = {"timings": tm, "points": P, "plain_cells": int(mask.sum()),
             "plain_fraction": float(mask.mean()), "training_cells": int(train_idx.size),
-            "final_flagged": int(flagged.size)}
+            "final_flagged": int(flagged.size), "marked": int(marked.size)}
     if probe is not None:
         mean, std = net.predict(torch.from_numpy(spec.coords(np.asarray(probe))).cuda())
         info["probe_mean"], info["probe_std"] = mean.cpu().numpy(), std.cpu().numpy()

@@ -46,3 +46,18 @@ def test_unknown_rule_is_an_error():
     import pytest
     with pytest.raises(ValueError):
         _flags(_t([[0, 0, 0]]), _t([[0, 0, 0]]), RefineConfig(rule="nope"))
+
+
+def test_contradiction_blocks():
+    from chaos_oneapi_b200.surrogate import _blocks
+    n1, n2 = 10, 12
+    cells = np.array([0 * n2 + 0, 5 * n2 + 6])
+    got = _blocks(cells, (n1, n2), 1)
+    want = set()
+    for a, b in ((0, 0), (5, 6)):
+        for da in (-1, 0, 1):
+            for db in (-1, 0, 1):
+                if 0 <= a + da < n1 and 0 <= b + db < n2:
+                    want.add((a + da) * n2 + b + db)
+    assert set(got.tolist()) == want and len(got) == len(want)
+    assert _blocks(np.zeros(0, dtype=np.int64), (n1, n2), 3).size == 0
