@@ -1,9 +1,10 @@
 """Generates tests/golden/reference_fixed.npz, reference_dopri.npz and
 reference_config1.npz from the reference's own sources built for the host
-(oracle/_ref/libchaos_ref.so; recipe in oracle/Makefile).  Run where the
+(oracle/_ref/libchaos_ref.so; recipe in oracle/Makefile), and
+oracle_rossler_cells.npz from the oracle's restatement.  Run where the
 reference tree is available:
 
-    python tests/golden/make_golden.py [--only fixed|dopri|program|config1]
+    python tests/golden/make_golden.py [--only fixed|dopri|program|config1|rossler_cells]
 
 Each case is one model x method on a few seeded points with short phase
 times (for the map model, iteration counts; maps have no QR branch); the
@@ -128,6 +129,34 @@ def config1_cells():
     print("wrote reference_config1.npz")
 
 
+# Regular cells of the 1024 x 1024 Rossler map of the precision form (a in
+# [0.05, 0.45], c in [2, 12], b = 0.2, x0 = (1, 1, 0) + U(-1e-3, 1e-3) seed
+# 0, transient 500, average 5000, renormalisation every 2) where the FP32
+# form once missed 1e-3: the FP64 oracle's answers at rtol 1e-12 (the
+# truth) and 1e-11 (its own reproducibility), and the oracle's Dopri5 at the
+# form's rtol 1e-6 (the method's own error at that tolerance).  These come
+# from the oracle's restatement (itself pinned to the reference), not from
+# the reference, which has no adaptive integrator.
+ROSSLER_CELLS = [14999, 23534, 291316, 563030, 156367, 481873, 196217, 630673]
+
+
+def rossler_cells():
+    params = oracle.make_grid(3, [0.2, 0.2, 5.7], [0, 0.05, 0.45, 1024], [2, 2.0, 12.0, 1024])
+    inits = oracle.make_inits(3, params.shape[0], [1.0, 1.0, 0.0], 1e-3, 0, 0)
+    idx = np.array(ROSSLER_CELLS)
+    kw = dict(t_transient=500.0, t_avg=5000.0, dt_renorm=2.0, threads=8)
+    p, x = params[idx], inits[idx]
+    truth = oracle.adaptive("rossler", p, x, 3, integrator="dverk65", rtol=1e-12, atol=1e-12,
+                            **kw)[0]
+    self11 = oracle.adaptive("rossler", p, x, 3, integrator="dverk65", rtol=1e-11, atol=1e-11,
+                             **kw)[0]
+    method = oracle.adaptive("rossler", p, x, 3, integrator="dopri5", rtol=1e-6, atol=1e-6,
+                             **kw)[0]
+    np.savez_compressed(os.path.join(HERE, "oracle_rossler_cells.npz"), index=idx, params=p,
+                        inits=x, truth=truth, oracle_rtol11=self11, method_rtol6=method)
+    print("wrote oracle_rossler_cells.npz")
+
+
 def main(only=None):
     if only in (None, "program"):
         program_outputs()
@@ -135,6 +164,8 @@ def main(only=None):
         dopri_trajectories()
     if only in (None, "config1"):
         config1_cells()
+    if only in (None, "rossler_cells"):
+        rossler_cells()
     if only not in (None, "fixed"):
         return
     out = {}
@@ -157,5 +188,6 @@ def main(only=None):
 if __name__ == "__main__":
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["fixed", "dopri", "program", "config1"], default=None)
+    ap.add_argument("--only", choices=["fixed", "dopri", "program", "config1", "rossler_cells"],
+                    default=None)
     main(ap.parse_args().only)
