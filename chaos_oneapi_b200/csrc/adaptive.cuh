@@ -134,9 +134,26 @@ template <class S, class E, class... Rest>
 CL_HD E lin_acc(E acc, double c, E k, Rest... rest) {
   return lin_acc<S, E>(vfma(S(c), k, acc), rest...);
 }
+// FP64 pairs serve the latency-bound forms (a few points, each a long serial
+// chain of steps): their combinations run as two interleaved chains -- the
+// odd and the even terms -- added at the end, one instruction more for about
+// half the dependency depth.
+CL_HD double2 lin2_acc(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+template <class... Rest>
+CL_HD double2 lin2_acc(double2 a, double2 b, double c, double2 k, Rest... rest) {
+  return lin2_acc(b, vfma(c, k, a), rest...);  // alternate the two chains
+}
+template <class... Rest>
+CL_HD double2 lin2_pair(double c1, double2 k1, double c2, double2 k2, Rest... rest) {
+  return lin2_acc(vmul(c2, k2), vmul(c1, k1), rest...);
+}
 template <class S, class E, class... Rest>
 CL_HD E lin(double c, E k, Rest... rest) {
-  return lin_acc<S, E>(vmul(S(c), k), rest...);
+  if constexpr (std::is_same<E, double2>::value && sizeof...(Rest) >= 2) {
+    return lin2_pair(c, k, rest...);
+  } else {
+    return lin_acc<S, E>(vmul(S(c), k), rest...);
+  }
 }
 
 // Arithmetic of the error norm and the step-size controller: FP32 for the
