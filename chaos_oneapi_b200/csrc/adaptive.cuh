@@ -399,6 +399,27 @@ CL_HD double ctl_fma(double a, double b, double c) { return fma(a, b, c); }
 // Largest error mean square that counts as finite.
 template <class C> CL_HD C err2_limit() { return sizeof(C) == 4 ? C(3.4e38f) : C(1e300); }
 
+// An attempt whose error estimate is not finite.  From a finite point this
+// is an overflow: a step far beyond the stability bound, which the
+// controller proposes after a run of steps whose error vanished (a state
+// resting on a stable equilibrium, where FP32 rounds the derivative to
+// zero, lets the proposal grow by 5x per step).  The reference's controller
+// meets an infinite error with its largest reduction,
+// newStep = step / min(facc1, fac11 / safeFac) = step / 5
+// (cuda/tools/dopri.dp.cpp:134), and so does this one, for NaN as well: the
+// attempt is rejected with h / 5.  A point whose parameters or state are not
+// finite is not an overflow and ends with status 1.
+constexpr int kNonfiniteDiv = 5;
+template <class R, int NP, int N>
+CL_HD bool point_finite(const R (&p)[NP], const R (&x)[N]) {
+  bool ok = true;  // v - v is 0 for finite v, NaN for Inf and NaN
+#pragma unroll
+  for (int i = 0; i < NP; i++) ok = ok && (p[i] - p[i] == R(0));
+#pragma unroll
+  for (int j = 0; j < N; j++) ok = ok && (x[j] - x[j] == R(0));
+  return ok;
+}
+
 // The step-size controller of dopri.dp.cpp:46-138 after an attempted step of
 // length h with error mean square err2, in the log2 domain: with
 // l = log2 err, the reference's fac = err^expo1 facOld^-beta / safe clamped
@@ -879,8 +900,13 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
   const C err2 = attempt<M, K, R, INTEG>(L, h, joint, ctl_rtol<R>(c), ctl_atol<R>(c), x1, V1,
                                          kx1, kv1);
   if (!(err2 <= err2_limit<C>())) {  // NaN or an overflowed error norm
-    lane_finish(L, a, 1);
-    return kFinished;
+    if (!point_finite(L.p, L.x)) {
+      lane_finish(L, a, 1);
+      return kFinished;
+    }
+    L.h = h / (R)kNonfiniteDiv;
+    L.reject = true;
+    return kRunning;
   }
   R hnew;
   if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {

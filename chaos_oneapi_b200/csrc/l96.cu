@@ -462,8 +462,16 @@ __global__ void __launch_bounds__(WARPS * 32, 4) l96_kernel(const AdaptiveArgs a
       }
       const float nc = joint ? (float)(N * (1 + k)) : (float)N;
       const float err = sqrtf(warp_sum(err2) / nc);
-      if (!(err == err) || err > 3.0e38f) {
-        status = 1;
+      if (!(err == err) || err > 3.0e38f) {  // the other forms' rule (adaptive.cuh: point_finite)
+        bool fin = (w.F - w.F == 0.f) && (w.gam - w.gam == 0.f);
+#pragma unroll
+        for (int j = 0; j < C; j++) fin = fin && (w.x[j] - w.x[j] == 0.f);
+        if (!__all_sync(FULL, fin)) {
+          status = 1;
+        } else {
+          w.h = h / 5.0f;  // the controller's largest reduction
+          w.reject = true;
+        }
       } else {
         const float fac11 = exp2f(expo1 * __log2f(fmaxf(err, 1e-30f)));
         if (err <= 1.0f) {

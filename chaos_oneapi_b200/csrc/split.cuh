@@ -302,9 +302,14 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
   L.steps++;
   const C err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, ctl_rtol<R>(c),
                                             ctl_atol<R>(c), x1, v1, kx1, kv1);
-  if (!(err2 <= err2_limit<C>())) {
-    split_finish(L, a, g, 1);
-    return kFinished;
+  if (!(err2 <= err2_limit<C>())) {  // the one-lane form's rule (point_finite)
+    if (!point_finite(L.p, L.x)) {
+      split_finish(L, a, g, 1);
+      return kFinished;
+    }
+    L.h = h / (R)kNonfiniteDiv;
+    L.reject = true;
+    return kRunning;
   }
   R hnew;
   if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {

@@ -61,9 +61,14 @@ CL_HD void run_trajectory(const TrajectoryArgs &ta, int64_t pt) {
     L.steps++;
     const C err2 = attempt<M, K, R, INTEG>(L, h, false, ctl_rtol<R>(c), ctl_atol<R>(c), x1, V1,
                                            kx1, kv1);
-    if (!(err2 <= err2_limit<C>())) {
-      status = 1;
-      break;
+    if (!(err2 <= err2_limit<C>())) {  // the sweeps' rule (point_finite)
+      if (!point_finite(L.p, L.x)) {
+        status = 1;
+        break;
+      }
+      L.h = h / (R)kNonfiniteDiv;
+      L.reject = true;
+      continue;
     }
     R hnew;
     const bool accepted = control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew);

@@ -631,6 +631,24 @@ static int control(integ_t *s, double err, double h, double hmax, int *reject, d
   return 0;
 }
 
+/* An attempt whose error norm is not finite.  From a finite point it is an
+ * overflow (a step far beyond the stability bound, proposed after steps whose
+ * error vanished); the reference's controller meets an infinite error with
+ * its largest reduction, newStep = step / min(facc1, fac11 / safeFac) =
+ * step / 5 (cuda/tools/dopri.dp.cpp:134), and so does this one, for NaN as
+ * well.  A point whose parameters or state are not finite ends: returns 1
+ * then, else 0 with the retry length in *hnext. */
+static int nonfinite_error(const integ_t *s, const double *y, double h, int *reject,
+                           double *hnext) {
+  for (int i = 0; i < orc_model_nparams(s->cfg->model); i++)
+    if (!isfinite(s->p[i])) return 1;
+  for (int c = 0; c < s->n; c++)
+    if (!isfinite(y[c])) return 1;
+  *reject = 1;
+  *hnext = h / 5.0;
+  return 0;
+}
+
 /* Takes the attempted step: y <- y1 (and, for Dopri5, the FSAL derivative). */
 static void take_step(integ_t *s, double *y) {
   memcpy(y, s->y1, sizeof(double) * s->N);
@@ -653,7 +671,10 @@ static int integrate(integ_t *s, double *y, double len) {
     double err, hnew;
     s->steps++;
     try_step(s, y, h, &err);
-    if (!isfinite(err)) return 1;
+    if (!isfinite(err)) {
+      if (nonfinite_error(s, y, h, &reject, &s->h)) return 1;
+      continue;
+    }
     if (control(s, err, h, hmax, &reject, &hnew)) {
       take_step(s, y);
       t = clamped ? len : t + h;
@@ -687,7 +708,10 @@ int orc_dopri_trajectory(int model, const double *p, const double *x0, double h0
       double err, hnew;
       s.steps++;
       try_step(&s, y, h, &err);
-      if (!isfinite(err)) return 1;
+      if (!isfinite(err)) {
+        if (nonfinite_error(&s, y, h, &reject, &s.h)) return 1;
+        continue;
+      }
       ok = control(&s, err, h, hmax, &reject, &hnew);
       if (ok) {
         take_step(&s, y);

@@ -138,3 +138,31 @@ def test_statuses_lorenz96_warp(lib, orc, schedule):
     good = [i for i in range(8) if i not in want]
     assert (bst[good] == 0).all()
     np.testing.assert_allclose(bs[good], cs[good], rtol=0, atol=1e-4)
+
+
+@pytest.mark.parametrize("prec,integ,schedule", FORMS)
+def test_overflowing_attempts_are_rejected(lib, orc, prec, integ, schedule):
+    """A Lorenz point resting on its stable equilibrium C+ (sigma 19.81,
+    rho 8.60: one real eigenvalue near -21.7, a pair near -0.89 +- 6i).  The
+    error estimate vanishes there, the controller grows the step 5x per step
+    until an attempt overflows; that attempt is rejected with h / 5 (the
+    reference controller's answer to an infinite error) and the point
+    finishes with status 0 and the oracle's exponents (which, over 200 time
+    units, differ from the real parts of J(C+)'s eigenvalues by ~7e-3: the
+    eigenvectors are not orthogonal)."""
+    import torch
+    s, r, b = 19.809384164222877, 8.602150537634408, 8.0 / 3.0
+    q = np.sqrt(b * (r - 1))
+    params = np.tile([s, r, b], (32, 1))
+    inits = np.tile([q, q, r - 1], (32, 1))
+    kw = dict(model="lorenz", method="var", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-6,
+              t_transient=100.0, t_avg=200.0, dt_renorm=1.0, max_steps=2_000_000)
+    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, **kw) as sw:
+        spec, st = _sweep(lib, torch, sw, (params, inits, np.full(32, 200.0)))
+    assert (st == 0).all(), st
+    ref, rst, _ = orc.adaptive("lorenz", params[:1], inits[:1], 3, integrator="dverk65",
+                               rtol=1e-12, atol=1e-12, t_transient=100.0, t_avg=200.0,
+                               dt_renorm=1.0)
+    assert rst[0] == 0
+    np.testing.assert_allclose(spec, np.tile(ref[0], (32, 1)), rtol=0, atol=1e-3)
+    np.testing.assert_allclose(spec.sum(1), -(s + 1 + b), rtol=0, atol=1e-4)
