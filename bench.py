@@ -596,14 +596,15 @@ def oracle_runs(w, params, inits, k, idx, form_rtol, form_integrator):
     return out
 
 
-def accuracy_vs(spec, status, ref, rst, others=None):
+def accuracy_vs(spec, status, ref, rst, others=None, params=None):
     """Per-exponent error of `spec` against the oracle's `ref` on the points
     both integrated to the end (status 0), split by regime (chaotic: the
     oracle's lambda_1 > 0.01).  `others`: {name: (spec, status)} of the
     oracle's own other runs on the same cells, reported the same way on the
     regular cells, and the cells where they all agree with `ref` within 1e-3
     ("conditioned": the finite-time exponents there do not depend on rounding
-    or on the tolerance)."""
+    or on the tolerance).  `params`: the cells' parameters, to list the three
+    regular cells with the largest errors."""
     ok = (rst == 0) & (status == 0)
     d = np.abs(spec[ok] - ref[ok])
     chaotic = ref[ok][:, 0] > 0.01
@@ -623,6 +624,12 @@ def accuracy_vs(spec, status, ref, rst, others=None):
         "regime_sign_agreement": float((np.sign(spec[ok][:, 0] - 0.01) ==
                                         np.sign(ref[ok][:, 0] - 0.01)).mean()),
     }
+    if params is not None and (~chaotic).any():
+        reg = np.flatnonzero(ok)[~chaotic]
+        worst = reg[np.argsort(-d[~chaotic].max(axis=1))[:3]]
+        out["worst_regular"] = [{"params": [float(v) for v in params[i]],
+                                 "form": [round(float(v), 6) for v in spec[i]],
+                                 "oracle": [round(float(v), 6) for v in ref[i]]} for i in worst]
     if others:
         cond = ~chaotic
         for name, (osp, ost) in others.items():
@@ -709,6 +716,10 @@ def run_sweep_bench(a, w, rank, world, local):
         clk = clocks.stop()
     elapsed_ms = t_start.elapsed_time(t_end)
     kernel_ms = sum(e0.elapsed_time(e1) for e0, e1 in ev) / a.steps
+    # device time between the timed launches (the L2 flush and any idle time)
+    gaps_ms = [t_start.elapsed_time(ev[0][0])] + [ev[i][1].elapsed_time(ev[i + 1][0])
+                                                   for i in range(a.steps - 1)]
+    gaps_ms.append(ev[-1][1].elapsed_time(t_end))
     if world > 1:
         t = torch.tensor([elapsed_ms, kernel_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -816,7 +827,7 @@ def run_sweep_bench(a, w, rank, world, local):
                      "flops_per_joint_step": flops_per_step(w["model"], w["integrator"], k),
                      "flops_per_transient_step": flops_per_state_step(w["model"],
                                                                       w["integrator"]),
-                     "kernel_ms": kernel_ms},
+                     "kernel_ms": kernel_ms, "gaps_ms": [round(g, 3) for g in gaps_ms]},
         "e2e": e2e,
         "points": {"ok": int((status_np == 0).sum()), "escaped": int((status_np == 4).sum()),
                    "other": int(((status_np != 0) & (status_np != 4)).sum()),
@@ -858,7 +869,8 @@ def run_sweep_bench(a, w, rank, world, local):
         orc_rtol = w.get("oracle_rtol", 1e-12)
         line["accuracy"] = dict(vs=f"FP64 adaptive oracle, rtol=atol={orc_rtol:g} (CPU)",
                                 oracle_runs=ORACLE_RUNS if runs else None,
-                                **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs))
+                                **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs,
+                                              params[idx]))
         if plain is not None:
             line["vs_plain_fp64"]["accuracy"] = accuracy_vs(plain["spec"][idx],
                                                             plain["status"][idx], ref, rst)
@@ -925,7 +937,8 @@ def run_second_map(a, w, cl, torch, dev, stream, flush, local):
         ref, rst = runs.pop("truth")
         out["accuracy"] = dict(vs="FP64 adaptive oracle, rtol=atol=1e-12 (CPU)",
                                oracle_runs=ORACLE_RUNS,
-                               **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs))
+                               **accuracy_vs(spec_np[idx], status_np[idx], ref, rst, runs,
+                                             params[idx]))
     return out
 
 

@@ -786,13 +786,27 @@ CL_HD void lane_finish(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int statu
 }
 
 // Tangent basis = identity, start of the alignment / averaging phases.
+// Component j of tangent vector i at the start of the tangent phase: the
+// identity basis (cuda/lyapunov.dp.cpp:133-226 starts from I), tilted in the
+// FP32 forms by 1e-6 along every other axis.  Why: a stable equilibrium at
+// the origin (Lorenz at rho < 1) decays below FP32's smallest denormal during
+// the transient, the state becomes exactly zero, and the variational
+// equations split exactly into invariant subspaces (for Lorenz, the x-y
+// block and z); an axis-aligned vector then never acquires the component
+// along the slower direction and Gram-Schmidt reports the exponents out of
+// order.  In FP64 the state stays nonzero and rounding supplies that
+// component.  The tilt changes an exponent by about 1e-6 / t_avg.
+template <class R> CL_HD R tangent_init(int i, int j) {
+  return i == j ? R(1) : (sizeof(R) == 4 ? R(1e-6f) : R(0));
+}
+
 template <class M, int K, class R, int INTEG>
 CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
   constexpr int N = M::N;
 #pragma unroll
   for (int i = 0; i < K; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) L.V[i][j] = (i == j) ? R(1) : R(0);
+    for (int j = 0; j < N; j++) L.V[i][j] = tangent_init<R>(i, j);
   refresh_tangent_derivs(L);
   L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.t_phase = 0.0;

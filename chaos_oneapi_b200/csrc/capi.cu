@@ -107,7 +107,7 @@ struct chaos_lyap_handle {
   int sm_count = 0;
   int block = 0;
   int schedule = CHAOS_SCHED_PERSISTENT;
-  int variant = 0;  // register-cap variant of the FP32 kernels (autotuned)
+  int variant = 0;  // kernel variant (chaos_lyap_desc.variant; autotuned)
   cudaStream_t own_stream = nullptr;
   cudaStream_t last_stream = nullptr;
   unsigned long long *queue = nullptr;  // point counters: persistent sweep / batch segments
@@ -428,7 +428,7 @@ static int enqueue(chaos_lyap_handle *h, int64_t P, const double *params, double
       }
     }
     if (m->dim > 4) rc = chaos::launch_l96_warp(integ, prec, a, 0, s);
-    else if (split) rc = chaos::launch_split(m->id, integ, prec, a, block, s);
+    else if (split) rc = chaos::launch_split(m->id, integ, prec, a, block, variant, s);
     else rc = chaos::launch_adaptive(m->id, integ, prec, a, block, 0, variant, s);
   }
   if (rc == chaos::kErrUnsupported)
@@ -542,15 +542,17 @@ static int autotune(chaos_lyap_handle *h, int64_t P_full, int64_t sample, int64_
   const int blocks[] = {64, 128};
   const int scheds[] = {CHAOS_SCHED_DIRECT, CHAOS_SCHED_PERSISTENT, CHAOS_SCHED_SPLIT_DIRECT,
                         CHAOS_SCHED_SPLIT_PERSISTENT};
-  const int nvar = h->d.precision == CHAOS_PREC_FP32 ? 2 : 1;
+  const bool fp32 = h->d.precision == CHAOS_PREC_FP32;
   float best = 1e30f;
   int best_b = h->block, best_s = h->schedule, best_v = h->variant, rc = CHAOS_LYAP_OK;
   cudaStream_t s = h->own_stream;
-  for (int v = 0; v < nvar && rc == CHAOS_LYAP_OK; v++)
+  for (int v = 0; v < 2 && rc == CHAOS_LYAP_OK; v++)
     for (int b : blocks)
       for (int sc : scheds) {
-        // the register-cap variants exist for the one-lane forms only
-        if (v > 0 && (sc == CHAOS_SCHED_SPLIT_DIRECT || sc == CHAOS_SCHED_SPLIT_PERSISTENT)) continue;
+        // variant 1: the register cap of the FP32 one-lane forms, the
+        // exchange layout of the FP64 split forms of 3-dimensional models
+        const bool split = sc == CHAOS_SCHED_SPLIT_DIRECT || sc == CHAOS_SCHED_SPLIT_PERSISTENT;
+        if (v > 0 && (split ? (fp32 || h->model->dim != 3) : !fp32)) continue;
         float ms = 0;
         for (int rep = 0; rep < 2 && rc == CHAOS_LYAP_OK; ++rep) {
           cudaEventRecord(e0, s);

@@ -131,9 +131,10 @@ inline cudaError_t launch_with_priority(void (*kern)(Args...), unsigned grid, un
   return cudaLaunchKernelEx(&cfg, kern, args...);
 }
 
-// Split form (split.cu): one point per group of four lanes.
+// Split form (split.cu): one point per group of four lanes; variant 1 is the
+// exchange layout of the FP64 form for 3-dimensional models.
 int launch_split(int model, int integrator, int precision, const AdaptiveArgs &a, int block,
-                 cudaStream_t s);
+                 int variant, cudaStream_t s);
 int launch_batch_split(int integrator, int precision, const BatchArgs &b, int block,
                        cudaStream_t s, double share = 1.0, bool high_priority = false);
 

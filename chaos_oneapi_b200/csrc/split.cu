@@ -1,6 +1,7 @@
 // Kernels of the split form (split.cuh): a sweep over one model and a mixed
 // batch, both with one parameter point per group of four lanes.
 #include <algorithm>
+#include <type_traits>
 
 #include "split.cuh"
 
@@ -23,11 +24,11 @@ __device__ __forceinline__ int64_t group_next_point(const AdaptiveArgs &a, const
 // Direct form: group i integrates point i.  Persistent form: groups pull
 // points from the queue until it is empty.  Gram-Schmidt is voted per warp,
 // as in the one-lane form.
-template <class M, class R, int INTEG>
+template <class M, class R, int INTEG, bool XCH>
 __global__ void __launch_bounds__(128) split_kernel(const AdaptiveArgs a) {
   const Group g = group_of();
   const Ctl c = make_ctl<R>(a);
-  SplitLane<M, R, INTEG> L;
+  SplitLane<M, R, INTEG, XCH> L;
   int64_t pt = a.queue ? group_next_point(a, g)
                        : ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kSplitLanes;
   bool active = pt < a.P;
@@ -50,10 +51,16 @@ __global__ void __launch_bounds__(128) split_kernel(const AdaptiveArgs a) {
   }
 }
 
+// variant 1: the exchange layout (split.cuh: XCH), FP64 and 3-dimensional
+// models only; otherwise the default layout.
 template <class M, class R, int INTEG>
-int launch_split_mri(const AdaptiveArgs &a, int block, cudaStream_t s) {
+int launch_split_mri(const AdaptiveArgs &a, int block, int variant, cudaStream_t s) {
   if (a.k != M::N) return kErrUnsupported;
-  auto kern = split_kernel<M, R, INTEG>;
+  constexpr bool xch_ok = std::is_same<R, double>::value && M::N == 3;
+  void (*kern)(AdaptiveArgs) = split_kernel<M, R, INTEG, false>;
+  if constexpr (xch_ok) {
+    if (variant == 1) kern = split_kernel<M, R, INTEG, true>;
+  }
   unsigned grid;
   const int64_t groups_per_block = block / kSplitLanes;
   const int64_t need = (a.P + groups_per_block - 1) / groups_per_block;
@@ -71,13 +78,14 @@ int launch_split_mri(const AdaptiveArgs &a, int block, cudaStream_t s) {
 }
 
 template <class M>
-int launch_split_m(int integ, int prec, const AdaptiveArgs &a, int block, cudaStream_t s) {
+int launch_split_m(int integ, int prec, const AdaptiveArgs &a, int block, int variant,
+                   cudaStream_t s) {
   if (integ == kDverk65) {
-    if (prec == kFP64) return launch_split_mri<M, double, kDverk65>(a, block, s);
-    if (prec == kFP32) return launch_split_mri<M, float, kDverk65>(a, block, s);
+    if (prec == kFP64) return launch_split_mri<M, double, kDverk65>(a, block, variant, s);
+    if (prec == kFP32) return launch_split_mri<M, float, kDverk65>(a, block, variant, s);
   } else if (integ == kDopri5) {
-    if (prec == kFP64) return launch_split_mri<M, double, kDopri5>(a, block, s);
-    if (prec == kFP32) return launch_split_mri<M, float, kDopri5>(a, block, s);
+    if (prec == kFP64) return launch_split_mri<M, double, kDopri5>(a, block, variant, s);
+    if (prec == kFP32) return launch_split_mri<M, float, kDopri5>(a, block, variant, s);
   }
   return kErrUnsupported;
 }
@@ -154,17 +162,17 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 2)
 
 }  // namespace adaptive
 
-int launch_split(int model, int integ, int prec, const AdaptiveArgs &a, int block,
+int launch_split(int model, int integ, int prec, const AdaptiveArgs &a, int block, int variant,
                  cudaStream_t s) {
   using namespace adaptive;
   if (a.P <= 0) return 0;
   if (block <= 0 || block > kMaxLaneBlock || block % 32) block = 64;
   switch (model) {
-    case kShimizu: return launch_split_m<Shimizu>(integ, prec, a, block, s);
-    case kLorenz: return launch_split_m<Lorenz>(integ, prec, a, block, s);
-    case kRossler: return launch_split_m<Rossler>(integ, prec, a, block, s);
-    case kChua: return launch_split_m<Chua>(integ, prec, a, block, s);
-    case kHyperRossler: return launch_split_m<HyperRossler>(integ, prec, a, block, s);
+    case kShimizu: return launch_split_m<Shimizu>(integ, prec, a, block, variant, s);
+    case kLorenz: return launch_split_m<Lorenz>(integ, prec, a, block, variant, s);
+    case kRossler: return launch_split_m<Rossler>(integ, prec, a, block, variant, s);
+    case kChua: return launch_split_m<Chua>(integ, prec, a, block, variant, s);
+    case kHyperRossler: return launch_split_m<HyperRossler>(integ, prec, a, block, variant, s);
     default: return kErrUnsupported;
   }
 }

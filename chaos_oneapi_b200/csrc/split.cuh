@@ -52,7 +52,44 @@ __device__ __forceinline__ float group_max(float e, unsigned mask) {
   return e;
 }
 
-template <class M, class R, int INTEG>
+// Exchange layout (XCH, FP64 and 3-dimensional models): lane 0 of the group
+// advances the state alone and lane 1 + q tangent vector q; at every stage
+// the vector lanes take the state's stage point from lane 0 (three FP64
+// shuffles) for their Jacobian.  Each lane then combines 3 rows per stage
+// instead of 6: on B200 an FP64 instruction holds its pipe for two cycles, so
+// the redundant state rows of the default layout are the longer part of a
+// step, while the default layout suits FP32, whose packed FFMA2 advances
+// state and vector rows in one instruction.  The state is broadcast to the
+// vector lanes after every accepted step (they need it for the Jacobian at
+// the start of a tangent phase and after Gram-Schmidt, and for the escape
+// and finiteness checks that every lane makes alike).
+template <bool XCH> __device__ __forceinline__ int vec_of(const Group &g) {
+  return XCH ? g.r - 1 : g.r;  // the tangent vector this lane carries (< 0: none)
+}
+
+template <class M>
+struct ExchangeStages {
+  const double *p;
+  unsigned mask;
+  int base;
+  bool state_lane;
+  CL_HD void operator()(int, const double *arg, double *out) const {
+    constexpr int N = M::N;
+    double X[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+#ifdef __CUDA_ARCH__
+      X[j] = __shfl_sync(mask, arg[j], base);
+#else
+      X[j] = arg[j];
+#endif
+    }
+    if (state_lane) M::f(X, out, p);
+    else M::jv(arg, out, p, X);
+  }
+};
+
+template <class M, class R, int INTEG, bool XCH = false>
 struct SplitLane {
   static constexpr int N = M::N;
   R p[M::NP];
@@ -69,8 +106,8 @@ struct SplitLane {
   int64_t steps;
 };
 
-template <class M, class R, int INTEG>
-__device__ __forceinline__ void split_flush(SplitLane<M, R, INTEG> &L) {
+template <class M, class R, int INTEG, bool XCH>
+__device__ __forceinline__ void split_flush(SplitLane<M, R, INTEG, XCH> &L) {
   Cold &c = cold_slot();
   const double y = log(L.prod) - c.comp[0];
   const double s = c.sum[0] + y;
@@ -79,14 +116,15 @@ __device__ __forceinline__ void split_flush(SplitLane<M, R, INTEG> &L) {
   L.prod = 1.0;
 }
 
-template <class M, class R, int INTEG>
-__device__ void split_finish(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Group &g,
+template <class M, class R, int INTEG, bool XCH>
+__device__ void split_finish(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a, const Group &g,
                              int status) {
   const Cold &c = cold_slot();
-  if (g.r < M::N) {
+  const int vi = vec_of<XCH>(g);
+  if (vi >= 0 && vi < M::N) {
     split_flush(L);
     const double lam = status ? quiet_nan() : c.sum[0] / c.t_avg;
-    a.spectrum.base[c.pt * a.spectrum.ps + g.r * a.spectrum.cs] = lam;
+    a.spectrum.base[c.pt * a.spectrum.ps + vi * a.spectrum.cs] = lam;
   }
   if (g.r == 0) {
     if (a.status) a.status[c.pt] = status;
@@ -94,12 +132,15 @@ __device__ void split_finish(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, c
   }
 }
 
-template <class M, class R, int INTEG>
-__device__ void split_start_tangent(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a,
+template <class M, class R, int INTEG, bool XCH>
+__device__ void split_start_tangent(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
                                     const Group &g) {
   constexpr int N = M::N;
 #pragma unroll
-  for (int j = 0; j < N; j++) L.v[j] = (j == g.r) ? R(1) : R(0);
+  for (int j = 0; j < N; j++) {  // rows of no vector stay zero
+    const int vi = vec_of<XCH>(g);
+    L.v[j] = (vi >= 0 && vi < M::N) ? tangent_init<R>(vi, j) : R(0);
+  }
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
   L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
   L.t_phase = 0.0;
@@ -113,8 +154,8 @@ __device__ void split_start_tangent(SplitLane<M, R, INTEG> &L, const AdaptiveArg
   }
 }
 
-template <class M, class R, int INTEG>
-__device__ void split_start(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt,
+template <class M, class R, int INTEG, bool XCH>
+__device__ void split_start(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a, int64_t pt,
                             const Group &g) {
   constexpr int N = M::N;
   Cold &cs = cold_slot();
@@ -147,8 +188,8 @@ __device__ void split_start(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, in
 
 // One step attempt: the state and this lane's vector; returns the group's
 // mean square weighted error (the same in all four lanes).
-template <class M, class R, int INTEG>
-__device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG> &st, R h,
+template <class M, class R, int INTEG, bool XCH>
+__device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG, XCH> &st, R h,
                                                    bool joint, bool has_vec, const Group &g,
                                                    typename CtlReal<R>::type rtol,
                                                    typename CtlReal<R>::type atol,
@@ -158,7 +199,31 @@ __device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG> 
   constexpr int N = M::N;
   constexpr int S = (INTEG == kDverk65) ? 8 : 7;
   C es = C(0), ev = C(0);
-  if constexpr (std::is_same<R, float>::value) {  // (state, v_r) as one packed pass
+  if constexpr (XCH) {  // this lane's rows: the state (lane 0) or its vector
+    static_assert(std::is_same<R, double>::value, "the exchange layout is the FP64 form's");
+    const bool state_lane = g.r == 0;
+    double yr[N], kr[N], y1r[N], k1r[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      yr[j] = state_lane ? st.x[j] : st.v[j];
+      kr[j] = state_lane ? st.kx[j] : st.kv[j];
+    }
+    double er = 0.0;
+    const ExchangeStages<M> fa{st.p, g.mask, g.base, state_lane};
+    if (INTEG == kDverk65) dverk_pass<N, double>(yr, h, fa, y1r, er, rtol, atol);
+    else dopri_pass<N, double>(yr, kr, h, fa, y1r, k1r, er, rtol, atol);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      x1[j] = __shfl_sync(g.mask, y1r[j], g.base);
+      v1[j] = state_lane ? 0.0 : y1r[j];
+      if (INTEG == kDopri5) {
+        kx1[j] = state_lane ? k1r[j] : 0.0;
+        kv1[j] = state_lane ? 0.0 : k1r[j];
+      }
+    }
+    es = state_lane ? er : C(0);
+    ev = state_lane ? C(0) : er;
+  } else if constexpr (std::is_same<R, float>::value) {  // (state, v_r) as one packed pass
     float X[S][N];
     float2 ya[N], ka[N], ya1[N], ka1[N];
 #pragma unroll
@@ -214,12 +279,13 @@ __device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG> 
 
 // Gram-Schmidt over the group in FP64 (see the header); false on a
 // degenerate basis (the same answer in all four lanes).
-template <class M, class R, int INTEG>
-__device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a,
+template <class M, class R, int INTEG, bool XCH>
+__device__ bool split_gram_schmidt(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
                                    const Ctl &c, const Group &g) {
   constexpr int N = M::N;
   constexpr int k = M::N;  // launches take k == dim
-  const bool has_vec = g.r < k;
+  const int vi = vec_of<XCH>(g);
+  const bool has_vec = vi >= 0 && vi < k;
   double vo[N], w[N];
   R before = 0;
 #pragma unroll
@@ -232,7 +298,7 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
   float cancel = 1.0f;
 #pragma unroll
   for (int q = 0; q < k; q++) {
-    if (g.r == q) {
+    if (vi == q) {
       double s = 0;
 #pragma unroll
       for (int j = 0; j < N; j++) s = fma(w[j], w[j], s);
@@ -245,8 +311,8 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
     }
     double qv[N];
 #pragma unroll
-    for (int j = 0; j < N; j++) qv[j] = __shfl_sync(g.mask, w[j], g.base + q);
-    if (g.r > q) {
+    for (int j = 0; j < N; j++) qv[j] = __shfl_sync(g.mask, w[j], g.base + q + (XCH ? 1 : 0));
+    if (vi > q) {
       double cq = 0;
       if (a.gs == 1) {  // modified: against the updated vector
 #pragma unroll
@@ -280,8 +346,8 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG> &L, const AdaptiveArgs
 
 // One step attempt of the group, phase bookkeeping included (the one-lane
 // form's lane_step, with the group's error norm and Gram-Schmidt).
-template <class M, class R, int INTEG>
-__device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c,
+template <class M, class R, int INTEG, bool XCH>
+__device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a, const Ctl &c,
                           const Group &g) {
   using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
@@ -297,7 +363,8 @@ __device__ int split_step(SplitLane<M, R, INTEG> &L, const AdaptiveArgs &a, cons
   const bool clamped = (double)L.h >= remaining;
   const R h = clamped ? (R)remaining : L.h;
   const bool joint = L.phase != kTransient;
-  const bool has_vec = g.r < M::N;  // launches take k == dim
+  const int vi = vec_of<XCH>(g);
+  const bool has_vec = vi >= 0 && vi < M::N;  // launches take k == dim
   R x1[N], v1[N], kx1[N], kv1[N];
   L.steps++;
   const C err2 = split_attempt<M, R, INTEG>(L, h, joint, has_vec, g, ctl_rtol<R>(c),

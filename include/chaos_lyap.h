@@ -115,8 +115,11 @@ typedef struct chaos_lyap_desc {
   int32_t device;           /* CUDA device ordinal */
   int32_t schedule;         /* CHAOS_SCHED_* */
   int32_t block;            /* threads per block, 0 = tuned default */
-  int32_t variant;          /* FP32 kernels: 0 = 128-register build, 1 = 96-register
-                               build (more resident warps, a few spills); autotuned */
+  int32_t variant;          /* 0 = default.  1 = FP32 one-lane kernels: the 96-register
+                               build (more resident warps, a few spills); FP64 split
+                               kernels of 3-dimensional models: the exchange layout
+                               (the state in one lane of the group, the vectors in the
+                               others); autotuned */
   double escape;            /* adaptive: escape radius of the state (0: 1e4) */
   int32_t reserved[4];
 } chaos_lyap_desc;
@@ -263,7 +266,7 @@ int chaos_lyap_trajectory(chaos_lyap_handle *h, int64_t P, const double *params,
                           const double *inits, int32_t nsteps, double *t_out, double *h_out,
                           double *x_out, int32_t *status, void *stream);
 
-/* The FP32 kernel variant in use (desc.variant, or the autotuner's choice). */
+/* The kernel variant in use (desc.variant, or the autotuner's choice). */
 int chaos_lyap_get_variant(chaos_lyap_handle *h, int32_t *variant);
 
 /* Drop-in for the reference launcher cudaLyapunov (cuda/lyapunov.dp.hpp:10-17)

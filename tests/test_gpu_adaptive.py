@@ -90,20 +90,21 @@ def test_fp32_rossler_vs_fp64_oracle(lib, orc):
     assert err[:, 0].max() < 0.05 and err[:, 1].max() < 0.05 and err.max() < 1.0, err.max(axis=0)
 
 
-@pytest.mark.parametrize("schedule", ["direct", "split"])
-def test_plain_fp64_sweep_matches_reference_config1_cells(lib, schedule):
+@pytest.mark.parametrize("schedule,variant", [("direct", 0), ("split", 0), ("split", 1)])
+def test_plain_fp64_sweep_matches_reference_config1_cells(lib, schedule, variant):
     """The plain FP64 sweep (DVERK 6(5), rtol = atol = 1e-10) of the 64 x 64
     Lorenz map against the reference's own VAR method at a fixed step of
     1e-4 on eight of its regular cells (tests/golden/reference_config1.npz,
     written by the reference's sources): within 1e-4 on every exponent --
     the FP64 path's correctness bar -- and, on the six fixed-point cells,
     within 1e-7 (the FP64 oracle lands within 1e-9 there and within 5e-6 on
-    the two periodic cells)."""
+    the two periodic cells).  The split form runs in both layouts (variant 1:
+    the state in one lane of the group, the vectors in the other three)."""
     import os
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_config1.npz"))
     got, st, _ = _run(lib, "lorenz", g["params"], g["inits"], method="var", precision="fp64",
                       integrator="dverk65", rtol=1e-10, atol=1e-10, h=1e-3, t_transient=100.0,
-                      t_avg=1000.0, dt_renorm=1.0, schedule=schedule)
+                      t_avg=1000.0, dt_renorm=1.0, schedule=schedule, variant=variant)
     assert (st == 0).all()
     want = g["spectrum"]
     assert np.abs(got - want).max() <= 1e-4, np.abs(got - want).max(axis=1)

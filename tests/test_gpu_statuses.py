@@ -38,9 +38,12 @@ def _rossler(orc):
 
 KW = dict(model="rossler", method="var", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-4,
           t_transient=5.0, t_avg=20.0, dt_renorm=1.0, max_steps=300_000)
-FORMS = [("fp32", "dopri5", "direct"), ("fp32", "dopri5", "persistent"),
-         ("fp32", "dopri5", "split"), ("fp32", "dopri5", "split_persistent"),
-         ("fp64", "dverk65", "direct"), ("fp64", "dverk65", "split")]
+# (precision, integrator, schedule, variant); variant 1 of the FP64 split
+# forms is the exchange layout (the state in one lane, the vectors in three)
+FORMS = [("fp32", "dopri5", "direct", 0), ("fp32", "dopri5", "persistent", 0),
+         ("fp32", "dopri5", "split", 0), ("fp32", "dopri5", "split_persistent", 0),
+         ("fp64", "dverk65", "direct", 0), ("fp64", "dverk65", "split", 0),
+         ("fp64", "dverk65", "split", 1), ("fp64", "dopri5", "split_persistent", 1)]
 TOL = {"fp32": 2e-4, "fp64": 2e-6}
 
 
@@ -68,11 +71,12 @@ def _check(clean, bad, tol):
     np.testing.assert_allclose(bs[regular], cs[regular], rtol=0, atol=tol)
 
 
-@pytest.mark.parametrize("prec,integ,schedule", FORMS)
-def test_statuses_one_lane_and_split(lib, orc, prec, integ, schedule):
+@pytest.mark.parametrize("prec,integ,schedule,variant", FORMS)
+def test_statuses_one_lane_and_split(lib, orc, prec, integ, schedule, variant):
     import torch
     clean, bad = _rossler(orc)
-    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, **KW) as sw:
+    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, variant=variant,
+                   **KW) as sw:
         _check(_sweep(lib, torch, sw, clean), _sweep(lib, torch, sw, bad), TOL[prec])
 
 
@@ -121,12 +125,10 @@ def test_statuses_lorenz96_warp(lib, orc, schedule):
     bp[3, 1] = 5e4
     bt[5] = 1e6
     bx[6] += 2e4
-    # h0 = 1e-4 with gamma = 5e4: the stiff point's rejected attempts stay
-    # finite in FP32 (its stage values grow ~h gamma per stage, and the
-    # quadratic term squares them: from larger h gamma they overflow and the
-    # point ends as non-finite instead)
+    # the stiff point's first attempts (h gamma = 500) overflow in FP32: they
+    # are rejected with h / 5 each until the step falls below h_min
     kw = dict(model="lorenz96", method="var", integrator="dopri5", precision="fp32", k=40,
-              gs="mgs", rtol=1e-6, atol=1e-6, h=1e-4, h_min=1e-4, t_transient=2.0, t_avg=5.0,
+              gs="mgs", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-4, t_transient=2.0, t_avg=5.0,
               dt_renorm=0.5, max_steps=50_000, schedule=schedule)
     with lib.Sweep(**kw) as sw:
         cs, cst = _sweep(lib, torch, sw, (params, inits, tavg))
@@ -140,8 +142,8 @@ def test_statuses_lorenz96_warp(lib, orc, schedule):
     np.testing.assert_allclose(bs[good], cs[good], rtol=0, atol=1e-4)
 
 
-@pytest.mark.parametrize("prec,integ,schedule", FORMS)
-def test_overflowing_attempts_are_rejected(lib, orc, prec, integ, schedule):
+@pytest.mark.parametrize("prec,integ,schedule,variant", FORMS)
+def test_overflowing_attempts_are_rejected(lib, orc, prec, integ, schedule, variant):
     """A Lorenz point resting on its stable equilibrium C+ (sigma 19.81,
     rho 8.60: one real eigenvalue near -21.7, a pair near -0.89 +- 6i).  The
     error estimate vanishes there, the controller grows the step 5x per step
@@ -157,7 +159,8 @@ def test_overflowing_attempts_are_rejected(lib, orc, prec, integ, schedule):
     inits = np.tile([q, q, r - 1], (32, 1))
     kw = dict(model="lorenz", method="var", rtol=1e-6, atol=1e-6, h=1e-2, h_min=1e-6,
               t_transient=100.0, t_avg=200.0, dt_renorm=1.0, max_steps=2_000_000)
-    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, **kw) as sw:
+    with lib.Sweep(precision=prec, integrator=integ, schedule=schedule, variant=variant,
+                   **kw) as sw:
         spec, st = _sweep(lib, torch, sw, (params, inits, np.full(32, 200.0)))
     assert (st == 0).all(), st
     ref, rst, _ = orc.adaptive("lorenz", params[:1], inits[:1], 3, integrator="dverk65",
