@@ -374,7 +374,7 @@ def run_surrogate_bench(a, rank, world, local):
             "config": {"workload": "surrogate", "map": f"{n}x{n} Lorenz (sigma, rho)",
                        "plain": "DVERK 6(5) FP64 rtol 1e-10, T 100 + 1000, renorm 1",
                        "ensemble": "4 x MLP 16 Fourier features -> 128 -> 128 -> 128 -> 3, "
-                                   "SiLU, BF16 mma.sync, FP32 accumulate, Adam 1e-3",
+                                   "SiLU, BF16 tcgen05.mma, FP32 accumulate in TMEM, Adam 1e-3",
                        "rule": rule,
                        "rounds": cfg.rounds, "round_max_new": cfg.round_max_new,
                        "verify_step": cfg.verify_step, "mark_radius": cfg.mark_radius},
