@@ -1007,7 +1007,8 @@ def main():
                     help="surrogate: time the plain sweep on this many random cells and "
                          "extrapolate (0: time the whole map)")
     ap.add_argument("--variant", type=int, default=-1,
-                    help="FP32 kernel register variant; -1 = autotune")
+                    help="kernel variant (FP32 one-lane: 96-register build; FP64 split: "
+                         "exchange layout); -1 = autotune")
     # smaller cases of the same kernels (profiler captures, quick checks)
     ap.add_argument("--grid", type=int, default=0, help="cells per side instead of the workload's")
     ap.add_argument("--t-scale", type=float, default=1.0,

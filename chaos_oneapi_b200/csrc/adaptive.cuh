@@ -410,6 +410,15 @@ template <class C> CL_HD C err2_limit() { return sizeof(C) == 4 ? C(3.4e38f) : C
 // attempt is rejected with h / 5.  A point whose parameters or state are not
 // finite is not an overflow and ends with status 1.
 constexpr int kNonfiniteDiv = 5;
+
+// Every state component within the escape radius (status 4 otherwise: after
+// an accepted step, and for the initial state before the first attempt).
+template <class R, int N> CL_HD bool state_inside(const R (&x)[N], double escape) {
+  bool inside = true;
+#pragma unroll
+  for (int j = 0; j < N; j++) inside = inside && (fabs(x[j]) <= (R)escape);
+  return inside;
+}
 template <class R, int NP, int N>
 CL_HD bool point_finite(const R (&p)[NP], const R (&x)[N]) {
   bool ok = true;  // v - v is 0 for finite v, NaN for Inf and NaN
@@ -897,6 +906,10 @@ template <class M, int K, class R, int INTEG>
 CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c) {
   using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
+  if (L.steps == 0 && !state_inside(L.x, c.escape)) {
+    lane_finish(L, a, 4);
+    return kFinished;
+  }
   if (L.steps >= c.max_steps) {
     lane_finish(L, a, 3);
     return kFinished;
@@ -941,10 +954,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
     if (!clamped || hnew < h) L.h = hnew;  // else keep the unclamped proposal
     L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
     L.t_gs += (float)h;
-    bool inside = true;
-#pragma unroll
-    for (int j = 0; j < N; j++) inside = inside && (fabs(L.x[j]) <= (R)c.escape);
-    if (!inside) {
+    if (!state_inside(L.x, c.escape)) {
       lane_finish(L, a, 4);
       return kFinished;
     }

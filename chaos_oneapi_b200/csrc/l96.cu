@@ -418,8 +418,14 @@ __global__ void __launch_bounds__(WARPS * 32, 4) l96_kernel(const AdaptiveArgs a
   if (w.pt < a.P) start_point();
   while (w.pt < a.P) {
     int status = -1;  // -1: running
-    if (w.steps >= a.max_steps) status = 3;
-    else if (!((double)w.h >= hmin)) status = 2;
+    if (w.steps == 0) {  // an initial state outside the escape radius (adaptive.cuh: state_inside)
+      bool inside = true;
+#pragma unroll
+      for (int j = 0; j < C; j++) inside = inside && (fabsf(w.x[j]) <= esc);
+      if (!__all_sync(FULL, inside)) status = 4;
+    }
+    if (status < 0 && w.steps >= a.max_steps) status = 3;
+    if (status < 0 && !((double)w.h >= hmin)) status = 2;
     if (status < 0) {
       const double remaining = w.phase_len - w.t_phase;
       const bool clamped = (double)w.h >= remaining;

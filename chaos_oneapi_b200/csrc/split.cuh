@@ -351,6 +351,10 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
                           const Group &g) {
   using C = typename CtlReal<R>::type;
   constexpr int N = M::N;
+  if (L.steps == 0 && !state_inside(L.x, c.escape)) {
+    split_finish(L, a, g, 4);
+    return kFinished;
+  }
   if (L.steps >= c.max_steps) {
     split_finish(L, a, g, 3);
     return kFinished;
@@ -395,10 +399,7 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
     if (!clamped || hnew < h) L.h = hnew;
     L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
     L.t_gs += (float)h;
-    bool inside = true;
-#pragma unroll
-    for (int j = 0; j < N; j++) inside = inside && (fabs(L.x[j]) <= (R)c.escape);
-    if (!inside) {
+    if (!state_inside(L.x, c.escape)) {
       split_finish(L, a, g, 4);
       return kFinished;
     }

@@ -662,6 +662,9 @@ static int integrate(integ_t *s, double *y, double len) {
   const double hmax = s->cfg->hmax > 0 ? s->cfg->hmax : 1e300;
   double t = 0;
   int reject = 0;
+  if (s->steps == 0 && s->cfg->escape > 0) /* an initial state outside the escape radius */
+    for (int c = 0; c < s->n; c++)
+      if (!(fabs(y[c]) <= s->cfg->escape)) return 4;
   while (t < len) {
     if (s->steps >= s->cfg->max_steps) return 3;
     if (s->h < s->cfg->hmin) return 2;
