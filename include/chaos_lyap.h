@@ -45,7 +45,8 @@ enum {
   CHAOS_POINT_NONFINITE = 1,      /* NaN / Inf in the state or a log-norm */
   CHAOS_POINT_STEP_UNDERFLOW = 2, /* adaptive step fell below h_min */
   CHAOS_POINT_MAX_STEPS = 3,      /* per-point step budget exhausted */
-  CHAOS_POINT_ESCAPED = 4         /* a state component left |x| <= escape */
+  CHAOS_POINT_ESCAPED = 4         /* a state component outside |x| <= escape (after a
+                                     step, or the initial state) */
 };
 
 /* Methods: reference cuda/lyapunov.dp.cpp:5-129 (FD, slave trajectories),
