@@ -436,31 +436,38 @@ CL_HD bool point_finite(const R (&p)[NP], const R (&x)[N]) {
 // clamped to [log2 0.1, log2 5], and h_new = h 2^-lf.  Accepted (err <= 1):
 // returns true, hnew = the next proposal (at most hmax; after a rejection no
 // longer than h), lfac_old = max(l, log2 1e-4).  Rejected: returns false,
-// hnew = h / min(facc1, err^expo1 / safe).  R the state precision, C = its
-// controller precision (FP32 for FP32 states, FP64 for FP64 states).
-template <class R, int INTEG>
-CL_HD bool control(typename CtlReal<R>::type err2, R h, typename CtlReal<R>::type &lfac_old,
+// hnew = h / min(facc1, err^expo1 / safe).  R the state precision.
+// EXACT: the arithmetic in the error norm's precision (FP64 for FP64
+// states), so that a state trajectory's step sequence follows the
+// reference's dopriStep to rounding (trajectory.cuh).  Otherwise -- the
+// sweeps -- in FP32 with the hardware log2 / exp2: the controller only
+// picks the next step's length, and on B200 the FP64 form's log2 / exp2
+// chain was a fifth of a step's latency where a step is latency-bound.
+template <class R, int INTEG, bool EXACT = false>
+CL_HD bool control(typename CtlReal<R>::type err2_in, R h, typename CtlReal<R>::type &lfac_old,
                    bool &reject, double hmax, R &hnew) {
   using C = typename CtlReal<R>::type;
-  constexpr C beta = C(0.04);
-  constexpr C expo1 = (INTEG == kDverk65 ? C(1.0 / 6.0) : C(0.2)) - beta * C(0.75);
-  constexpr C log2_safe = C(-0.15200309344504995);   // log2 0.9
-  constexpr C log2_facc1 = C(2.321928094887362);     // log2 5
-  constexpr C log2_facc2 = C(-3.321928094887362);    // log2 0.1
-  const C lerr = C(0.5) * ctl_log2(err2 > C(1e-38f) ? err2 : C(1e-38f));
-  if (err2 <= C(1)) {
-    C lf = ctl_fma(expo1, lerr, ctl_fma(-beta, lfac_old, -log2_safe));
+  using T = typename std::conditional<EXACT, C, float>::type;
+  constexpr T beta = T(0.04);
+  constexpr T expo1 = (INTEG == kDverk65 ? T(1.0 / 6.0) : T(0.2)) - beta * T(0.75);
+  constexpr T log2_safe = T(-0.15200309344504995);   // log2 0.9
+  constexpr T log2_facc1 = T(2.321928094887362);     // log2 5
+  constexpr T log2_facc2 = T(-3.321928094887362);    // log2 0.1
+  const T err2 = (T)err2_in;  // beyond FP32's range: +inf, rejected with h / 5 below
+  const T lerr = T(0.5) * ctl_log2(err2 > T(1e-38f) ? err2 : T(1e-38f));
+  if (err2 <= T(1)) {
+    T lf = ctl_fma(expo1, lerr, ctl_fma(-beta, (T)lfac_old, -log2_safe));
     lf = lf < log2_facc2 ? log2_facc2 : lf;
     lf = lf < log2_facc1 ? lf : log2_facc1;
     R hn = h * (R)ctl_exp2(-lf);
-    lfac_old = lerr > log2_fac_min<C>() ? lerr : log2_fac_min<C>();
+    lfac_old = (C)(lerr > log2_fac_min<T>() ? lerr : log2_fac_min<T>());
     if ((double)hn > hmax) hn = (R)hmax;
     if (reject && hn > h) hn = h;
     reject = false;
     hnew = hn;
     return true;
   }
-  C lr = ctl_fma(expo1, lerr, -log2_safe);
+  T lr = ctl_fma(expo1, lerr, -log2_safe);
   lr = lr < log2_facc1 ? lr : log2_facc1;
   hnew = h * (R)ctl_exp2(-lr);
   reject = true;

@@ -270,11 +270,13 @@ __device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG, 
     es = ea.x;
     ev = ea.y;
   }
-  // the state's error once (lane 0), each vector's in its own lane
-  C e = (g.r == 0 ? es : C(0)) + ((joint && has_vec) ? ev : C(0));
+  // the state's error once (lane 0), each vector's in its own lane; summed
+  // over the group in FP32 (it only steers the controller, whose arithmetic
+  // is FP32 in the sweeps)
+  float e = (float)((g.r == 0 ? es : C(0)) + ((joint && has_vec) ? ev : C(0)));
   e = group_sum(e, g.mask);
-  const C inv_nc = joint ? C(1) / C(N * (1 + M::N)) : C(1) / C(N);
-  return e * inv_nc;
+  const float inv_nc = joint ? 1.0f / float(N * (1 + M::N)) : 1.0f / float(N);
+  return (C)(e * inv_nc);
 }
 
 // Gram-Schmidt over the group in FP64 (see the header); false on a
@@ -330,9 +332,9 @@ __device__ bool split_gram_schmidt(SplitLane<M, R, INTEG, XCH> &L, const Adaptiv
 #pragma unroll
   for (int j = 0; j < N; j++) L.v[j] = has_vec ? (R)w[j] : R(0);
   cancel = group_max(cancel, g.mask);
-  double rmin = has_vec ? rr : 1.0;
-  rmin = fmin(rmin, __shfl_xor_sync(g.mask, rmin, 1));
-  rmin = fmin(rmin, __shfl_xor_sync(g.mask, rmin, 2));
+  float rmin = has_vec ? (float)fmin(rr, 1.0) : 1.0f;  // steers the interval only
+  rmin = fminf(rmin, __shfl_xor_sync(g.mask, rmin, 1));
+  rmin = fminf(rmin, __shfl_xor_sync(g.mask, rmin, 2));
   if (L.phase == kAverage && has_vec) {
     L.prod *= rr;
     if (!(L.prod < 1e150 && L.prod > 1e-150)) split_flush(L);

@@ -5,10 +5,10 @@
 // rejected attempts are retried inside the call -- leaving the next step's
 // proposal and the FSAL derivative for the following call.  Here one lane
 // makes `nsteps` such calls for its point and records, after each, the time,
-// the proposal and the state.  The step pass and the controller are the
-// sweep kernels' own (adaptive.cuh: attempt, control), so this is also how
-// their step sequence is compared with the reference's.  DVERK 6(5) runs
-// the same way with its own tableau and exponent.
+// the proposal and the state.  The step pass is the sweep kernels' own
+// (adaptive.cuh: attempt) and so is the controller, with its arithmetic in
+// FP64 for FP64 states (control<..., EXACT>; the sweeps evaluate it in
+// FP32).  DVERK 6(5) runs the same way with its own tableau and exponent.
 #pragma once
 #include "adaptive.cuh"
 
@@ -71,7 +71,7 @@ CL_HD void run_trajectory(const TrajectoryArgs &ta, int64_t pt) {
       continue;
     }
     R hnew;
-    const bool accepted = control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew);
+    const bool accepted = control<R, INTEG, true>(err2, h, L.lfac_old, L.reject, c.hmax, hnew);
     L.h = hnew;
     if (!accepted) continue;
     bool inside = true;
