@@ -489,8 +489,8 @@ CL_HD bool control(typename CtlReal<R>::type err2_in, R h, typename CtlReal<R>::
 // are relative to its length, and Gram-Schmidt keeps only the part of it not
 // along the earlier vectors, so they grow by the cancellation factor
 // |v_i| / r_i.  L adapts so that the log of that factor over one interval, at
-// the largest recent rate, stays near tau / 8 (measured: tighter targets no
-// longer change the trace identity or the FP32 spectra, looser ones do).
+// the largest recent rate, stays near tau / 4, and the norms shrink by at
+// most e^2 over one interval (renorm.cuh).
 template <class M, int K, class R, int INTEG>
 struct Lane {
   static constexpr int N = M::N;

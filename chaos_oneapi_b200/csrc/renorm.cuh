@@ -35,7 +35,7 @@ constexpr int kRenormSplitInit = 16, kRenormSplitMax = 64;
 // both bounded:
 //  * cancellation: errors in a vector are relative to its length, and
 //    Gram-Schmidt keeps only its part not along the earlier vectors, so they
-//    grow by |v_i| / r_i -- allowed up to exp(tau / 8);
+//    grow by |v_i| / r_i -- allowed up to exp(kCancelFrac tau) = exp(tau / 4);
 //  * shrinking: a vector in a contracting direction loses length, and once
 //    its components fall below atol / rtol the error control on it is
 //    absolute, not relative -- the norms may shrink by at most
@@ -48,9 +48,15 @@ constexpr int kRenormSplitInit = 16, kRenormSplitMax = 64;
 // part of an orbit does not open an interval that a contraction burst later
 // crosses), grows at most 2x per pass, and lies in [dt / 64, dt].  The rate
 // starts at the value that gives L = dt / 16 (initial_renorm_rate).
+// kCancelFrac: tau / 8 and tau / 4 give the same FP32 spectra on 512 Rossler
+// and 256 Lorenz cells of the 1024^2 maps against the FP64 oracle (regular
+// cells within 1e-3: 95.6 % and 91.2 % both; median errors within 10 %;
+// Lorenz trace identity, median 1.28e-5 -> 1.41e-5), with half the
+// Gram-Schmidt passes -- a third of a step's latency in the four-lane form.
 constexpr float kShrinkMax = 2.0f;
+constexpr float kCancelFrac = 0.25f;
 CL_HD float initial_renorm_rate(float tau, float dt) {
-  return 0.125f * tau * kRenormSplitInit / dt;
+  return kCancelFrac * tau * kRenormSplitInit / dt;
 }
 template <class T>
 CL_HD void next_renorm_interval(T &L, T &rate_max, float cancel, double rmin, T t_gs, float tau,
@@ -58,12 +64,13 @@ CL_HD void next_renorm_interval(T &L, T &rate_max, float cancel, double rmin, T 
   constexpr float ln2 = 0.6931471805599453f;
   const float cancel_strain = 0.5f * ln2 * fast_log2f(cancel);
   const float shrink_strain =
-      (0.125f * tau / kShrinkMax) * (-ln2) * fast_log2f(fminf((float)rmin, 1.0f));
+      (kCancelFrac * tau / kShrinkMax) * (-ln2) * fast_log2f(fminf((float)rmin, 1.0f));
   const float strain = fmaxf(cancel_strain, shrink_strain);
   const T rate = sizeof(T) == 4 ? (T)fast_div(strain, (float)t_gs) : (T)strain / t_gs;
   rate_max = rate > T(0.995) * rate_max ? rate : T(0.995) * rate_max;
   const T rm = rate_max > T(1e-30) ? rate_max : T(1e-30);
-  const T target = sizeof(T) == 4 ? (T)fast_div(0.125f * tau, (float)rm) : T(0.125) * tau / rm;
+  const T target = sizeof(T) == 4 ? (T)fast_div(kCancelFrac * tau, (float)rm)
+                                   : T(kCancelFrac) * tau / rm;
   const T lo = dt * T(1.0 / kRenormSplitMax);
   T next = target > lo ? target : lo;
   next = next < T(2) * L ? next : T(2) * L;
