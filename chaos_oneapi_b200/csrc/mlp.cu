@@ -369,6 +369,18 @@ __global__ void adam_kernel(float *p, const float *gr, float *m, float *v, bf16 
   pb[i] = __float2bfloat16(p[i]);
 }
 
+// Minibatch rows idx[0..B) of the training set (device xy N x 2, T N x outs
+// doubles) into the step's buffers, targets to FP32.
+__global__ void gather_batch_kernel(const int *idx, int64_t B, const double *xy, const double *T,
+                                    int outs, double *xyb, float *Tb) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= B) return;
+  const int64_t j = idx[r];
+  xyb[2 * r] = xy[2 * j];
+  xyb[2 * r + 1] = xy[2 * j + 1];
+  for (int c = 0; c < outs; c++) Tb[r * outs + c] = (float)T[j * outs + c];
+}
+
 __global__ void to_bf16_kernel(const float *p, bf16 *pb, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) pb[i] = __float2bfloat16(p[i]);
@@ -416,6 +428,8 @@ struct chaos_mlp {
   float *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *Y = nullptr, *dA = nullptr, *loss = nullptr;
   float *Tb = nullptr;
   double *xyb = nullptr;
+  int *idx = nullptr;      // minibatch row indices of kTrainChunk steps
+  int64_t idx_cap = 0;
   int *d_err = nullptr;  // set by a GEMM whose wait on the tensor core gave up
 };
 
@@ -649,6 +663,7 @@ int chaos_mlp_destroy(chaos_mlp *h) {
   DevGuard g(h->device);
   cudaDeviceSynchronize();
   free_ws(h);
+  cudaFree(h->idx);
   cudaFree(h->p);
   cudaFree(h->g);
   cudaFree(h->m);
@@ -759,18 +774,29 @@ int chaos_mlp_train(chaos_mlp *h, const double *xy, const double *T, int64_t N, 
                     int batch, float lr, uint64_t seed, void *stream, float *loss_out) {
   if (!h || !xy || !T || N <= 0 || steps < 0 || batch < 16)
     return fail(CHAOS_LYAP_EINVAL, "bad arguments");
+  if (N > INT32_MAX) return fail(CHAOS_LYAP_EINVAL, "at most 2^31 - 1 training rows");
   DevGuard g(h->device);
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t B = std::min<int64_t>(batch, N);
   int rc = ensure_ws(h, B);
   if (rc) return rc;
-  // targets to FP32 on the host once, gathered per batch (small: N x 3)
-  std::vector<double> xd(N * 2), td(N * h->outs);
-  cudaMemcpyAsync(xd.data(), xy, sizeof(double) * xd.size(), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(td.data(), T, sizeof(double) * td.size(), cudaMemcpyDeviceToHost, s);
-  cudaStreamSynchronize(s);
-  std::vector<int64_t> perm(N);
-  for (int64_t i = 0; i < N; i++) perm[i] = i;
+  // The minibatches are drawn on the host (a seeded Fisher-Yates shuffle per
+  // epoch), kTrainChunk steps of row indices at a time, and gathered on the
+  // device from the training set where it lies: a step is three kernels
+  // and a copy of nothing, and the host never waits for the GPU until the
+  // end (each index chunk is copied on the stream, after the steps that read
+  // the previous one).
+  constexpr int kTrainChunk = 256;
+  if (h->idx_cap < kTrainChunk * B) {
+    cudaFree(h->idx);
+    h->idx = nullptr;
+    h->idx_cap = 0;
+    cudaError_t e = cudaMalloc((void **)&h->idx, sizeof(int) * kTrainChunk * B);
+    if (e != cudaSuccess) return fail(CHAOS_LYAP_ENOMEM, std::string("batch indices: ") + cudaGetErrorString(e));
+    h->idx_cap = kTrainChunk * B;
+  }
+  std::vector<int> perm(N);
+  for (int64_t i = 0; i < N; i++) perm[i] = (int)i;
   uint64_t st = seed * 0x9E3779B97F4A7C15ULL + 1;
   auto rnd = [&]() {
     st ^= st << 13;
@@ -779,31 +805,34 @@ int chaos_mlp_train(chaos_mlp *h, const double *xy, const double *T, int64_t N, 
     return st;
   };
   int64_t pos = N;
-  std::vector<double> bx(B * 2);
-  std::vector<float> bt(B * h->outs);
+  std::vector<int> chunk(kTrainChunk * B);
   const int64_t n = h->np * h->E;
-  for (int it = 0; it < steps; it++) {
-    for (int64_t r = 0; r < B; r++) {
-      if (pos >= N) {  // new epoch: Fisher-Yates shuffle
+  for (int it0 = 0; it0 < steps; it0 += kTrainChunk) {
+    const int cs = std::min(kTrainChunk, steps - it0);
+    for (int64_t r = 0; r < cs * B; r++) {
+      if (pos >= N) {  // new epoch
         for (int64_t i = N - 1; i > 0; i--) std::swap(perm[i], perm[rnd() % (uint64_t)(i + 1)]);
         pos = 0;
       }
-      const int64_t j = perm[pos++];
-      bx[2 * r] = xd[2 * j];
-      bx[2 * r + 1] = xd[2 * j + 1];
-      for (int c = 0; c < h->outs; c++) bt[r * h->outs + c] = (float)td[j * h->outs + c];
+      chunk[r] = perm[pos++];
     }
-    cudaMemcpyAsync(h->xyb, bx.data(), sizeof(double) * B * 2, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(h->Tb, bt.data(), sizeof(float) * B * h->outs, cudaMemcpyHostToDevice, s);
-    rc = grad_step(h, h->xyb, h->Tb, B, s);
-    if (rc) return cuda_fail((cudaError_t)rc, "train step");
-    h->t++;
-    const float b1 = 0.9f, b2 = 0.999f;
-    const float c1 = 1.f / (1.f - std::pow(b1, (float)h->t));
-    const float c2 = 1.f / (1.f - std::pow(b2, (float)h->t));
-    adam_kernel<<<blocks(n, 256), 256, 0, s>>>(h->p, h->g, h->m, h->v, h->pb, n, lr, b1, b2, 1e-8f, c1, c2);
-    // the host buffers are reused next step: wait for the copies to be consumed
-    cudaStreamSynchronize(s);
+    // pageable source: staged before the call returns, so the vector can be
+    // refilled while the copy and the steps before it are still queued
+    cudaError_t e = cudaMemcpyAsync(h->idx, chunk.data(), sizeof(int) * cs * B,
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "batch indices");
+    for (int k = 0; k < cs; k++) {
+      gather_batch_kernel<<<blocks(B, 256), 256, 0, s>>>(h->idx + (int64_t)k * B, B, xy, T, h->outs,
+                                                         h->xyb, h->Tb);
+      rc = grad_step(h, h->xyb, h->Tb, B, s);
+      if (rc) return cuda_fail((cudaError_t)rc, "train step");
+      h->t++;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float c1 = 1.f / (1.f - std::pow(b1, (float)h->t));
+      const float c2 = 1.f / (1.f - std::pow(b2, (float)h->t));
+      adam_kernel<<<blocks(n, 256), 256, 0, s>>>(h->p, h->g, h->m, h->v, h->pb, n, lr, b1, b2,
+                                                 1e-8f, c1, c2);
+    }
   }
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "train");
