@@ -128,22 +128,85 @@ __device__ __forceinline__ int core_offset(int r, int k) {
 }
 
 // Gathers rows [row0, row0 + nrows) x k [k0, k0 + 64) of an operand X(row, k)
-// = X[row * srow + k * sk] into a stage (zero outside rows < rmax, k < kmax),
-// walking the contiguous index fastest.
+// = X[row * srow + k * sk] into a stage (zero outside rows < rmax, k < kmax).
+// nrows is a multiple of 16.  Three ways, by the operand's layout:
+//  * k contiguous (sk = 1, rows 16-byte aligned): 16-byte loads of 8
+//    consecutive k, stored whole as one row of a core matrix;
+//  * rows contiguous (srow = 1, k 16-byte aligned): 16-byte loads of 8
+//    consecutive rows at one k, scattered into the 8 rows of a core matrix
+//    (threads of a warp take consecutive k, so a warp's stores spread over
+//    four core matrices);
+//  * otherwise element by element.
+// Each thread issues its loads for several chunks before it stores any, so
+// the loads of a stage overlap instead of waiting one after another.
 __device__ __forceinline__ void gather_stage(bf16 *dst, const bf16 *src, int nrows, int row0,
                                              int rmax, int64_t srow, int k0, int kmax,
                                              int64_t sk) {
   const bf16 zero = __float2bfloat16(0.f);
-  const int total = nrows * kTcK;
-  if (sk == 1) {
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int r = e >> 6, kk = e & 63;
-      const int row = row0 + r, k = k0 + kk;
-      dst[core_offset(r, kk)] = (row < rmax && k < kmax) ? src[row * srow + k] : zero;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+  constexpr int U = 4;  // chunks in flight per thread
+  if (sk == 1 && aligned && srow % 8 == 0) {
+    const int chunks = nrows * (kTcK / 8);
+    for (int c0 = threadIdx.x; c0 < chunks; c0 += U * blockDim.x) {
+      uint4 v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = c0 + u * blockDim.x;
+        const int r = c >> 3, kk = (c & 7) << 3, row = row0 + r, k = k0 + kk;
+        v[u] = make_uint4(0, 0, 0, 0);
+        if (c < chunks && row < rmax) {
+          if (k + 8 <= kmax) {
+            v[u] = *reinterpret_cast<const uint4 *>(src + (int64_t)row * srow + k);
+          } else {
+            __align__(16) bf16 t[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) t[i] = (k + i < kmax) ? src[(int64_t)row * srow + k + i] : zero;
+            v[u] = *reinterpret_cast<const uint4 *>(t);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = c0 + u * blockDim.x;
+        if (c < chunks)
+          *reinterpret_cast<uint4 *>(dst + core_offset(c >> 3, (c & 7) << 3)) = v[u];
+      }
+    }
+  } else if (srow == 1 && aligned && sk % 8 == 0 && row0 % 8 == 0) {
+    const int chunks = (nrows / 8) * kTcK;  // (8-row group, k) pairs, k fastest
+    for (int c0 = threadIdx.x; c0 < chunks; c0 += U * blockDim.x) {
+      uint4 v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = c0 + u * blockDim.x;
+        const int kk = c % kTcK, r = (c / kTcK) * 8, row = row0 + r, k = k0 + kk;
+        v[u] = make_uint4(0, 0, 0, 0);
+        if (c < chunks && k < kmax) {
+          if (row + 8 <= rmax) {
+            v[u] = *reinterpret_cast<const uint4 *>(src + row + (int64_t)k * sk);
+          } else {
+            __align__(16) bf16 t[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) t[i] = (row + i < rmax) ? src[row + i + (int64_t)k * sk] : zero;
+            v[u] = *reinterpret_cast<const uint4 *>(t);
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int c = c0 + u * blockDim.x;
+        if (c < chunks) {
+          const int kk = c % kTcK, r = (c / kTcK) * 8;
+          const bf16 *t = reinterpret_cast<const bf16 *>(&v[u]);
+#pragma unroll
+          for (int i = 0; i < 8; i++) dst[core_offset(r + i, kk)] = t[i];
+        }
+      }
     }
   } else {
+    const int total = nrows * kTcK;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
-      const int r = e % nrows, kk = e / nrows;
+      const int r = e >> 6, kk = e & 63;
       const int row = row0 + r, k = k0 + kk;
       dst[core_offset(r, kk)] = (row < rmax && k < kmax) ? src[row * srow + k * sk] : zero;
     }
