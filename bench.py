@@ -998,7 +998,7 @@ def main():
                     help="lorenz1024: cells of the Rossler 1024^2 map checked against the oracle")
     ap.add_argument("--no-rossler", dest="with_rossler", action="store_false",
                     help="lorenz1024: skip the Rossler 1024^2 precision-form map timed beside it")
-    ap.add_argument("--verify-step", type=int, default=0,
+    ap.add_argument("--verify-step", type=int, default=8,
                     help="surrogate: subgrid step of the verification sweep (0: none)")
     ap.add_argument("--mark-radius", type=int, default=8,
                     help="surrogate: half-width of the block integrated around a contradiction")

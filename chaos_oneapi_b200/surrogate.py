@@ -225,8 +225,12 @@ class RefineConfig:
     # the map has structure the networks do not resolve (periodic windows
     # inside the chaotic region are bands a few cells wide): the final fill
     # integrates the (2 mark_radius + 1)^2 block of cells around every
-    # contradiction.  0 switches the stage off.
-    verify_step: int = 0
+    # contradiction.  0 switches the stage off.  Measured on the 4096^2
+    # Lorenz map (10,000 fresh held-out cells): without it 99.47 % regime
+    # agreement at 0.218x of the plain sweep's time, with (8, 8) 99.64 % at
+    # 0.184x -- the blocks it adds replace flagged cells the last rounds
+    # would have integrated one by one.
+    verify_step: int = 8
     mark_radius: int = 8
     seed: int = 0
     timings: dict = field(default_factory=dict)
