@@ -81,10 +81,41 @@ def test_refined_map_against_plain_on_held_out_cells(lib, rule):
     ok = st == 0
     agree = ((out[held, 0] > 0.01) == (truth[:, 0] > 0.01))[ok].mean()
     # the trained ensemble fills part of the map (the rest, flagged by the
-    # spread / near-zero rule, is integrated), and the regimes it fills agree
+    # spread / near-zero rule or marked by the verification sweep, is
+    # integrated), and the regimes it fills agree (measured: 0.996 under
+    # either rule with the default verification sweep)
     assert info["plain_fraction"] < 0.95, info
-    assert agree > 0.98, (agree, info)
+    assert agree > 0.99, (agree, info)
     filled = ok & ~mask[held]
     assert filled.sum() > 20
     assert np.median(np.abs(out[held][filled, 0] - truth[filled, 0])) < 0.05
+    sw.close()
+
+
+def test_verification_sweep_gains_regime_agreement(lib):
+    """The verification sweep (integrate a subgrid, mark blocks around the
+    cells where the plain result contradicts the ensemble's regime) on the
+    same 256 x 256 map: regime agreement on held-out cells with the sweep is
+    at least that without it (measured 0.996 against 0.988), at the price of
+    more integrated cells."""
+    from chaos_oneapi_b200.surrogate import MapSpec, RefineConfig, plain_sweep, refine_map
+    spec = MapSpec("lorenz", [10.0, 28.0, 8.0 / 3.0], [0, 5.0, 20.0, 256], [1, 0.0, 200.0, 256],
+                   [1.0, 1.0, 1.0], seed=4)
+    sw = lib.Sweep(model="lorenz", method="var", integrator="dverk65", precision="fp64",
+                   rtol=1e-8, atol=1e-8, h=1e-3, t_transient=20.0, t_avg=300.0, dt_renorm=1.0)
+    rng = np.random.default_rng(11)
+    held = rng.choice(256 * 256, 1000, replace=False)
+    truth, st = plain_sweep(sw, spec, held)
+    ok = st == 0
+    res = {}
+    for vs in (0, 8):
+        cfg = RefineConfig(train_grid=64, steps0=3000, steps_round=1500, rounds=2,
+                           round_grid_step=2, round_max_new=8192, rule="regime", lam_limit=0.005,
+                           verify_step=vs, mark_radius=8)
+        out, mask, info = refine_map(spec, sw, cfg)
+        agree = ((out[held, 0] > 0.01) == (truth[:, 0] > 0.01))[ok].mean()
+        res[vs] = (agree, info["plain_fraction"], info["timings"].get("verify"))
+    assert res[8][2] is not None and res[8][2]["cells"] > 0, res
+    assert res[8][0] >= res[0][0] and res[8][0] > 0.99, res
+    assert res[8][1] >= res[0][1], res
     sw.close()
