@@ -39,6 +39,7 @@ constexpr int N = 40;        // model dimension
 constexpr int G = 4;         // vectors processed at once per warp (lane groups)
 constexpr int C = 5;         // components per lane
 constexpr int WARPS = 4;     // warps (points) per block
+constexpr int PV = 4;        // Gram-Schmidt: later vectors per lane group per projection round
 constexpr unsigned FULL = 0xffffffffu;
 
 struct DPc {  // Dormand-Prince 5(4), cuda/tools/dopri.dp.cpp:14-44
@@ -276,20 +277,31 @@ __device__ double mgs_qr(Warp &w, const float *V, float *base, int k, int g, int
 #pragma unroll
       for (int j = 0; j < C; j++) W[q * N + li * C + j] = wq[j];
     }
-    // projections of the later vectors, four at a time
-    for (int j0 = q + 1; j0 < k; j0 += G) {
-      const int vj = j0 + g;
-      const bool valid = vj < k;
-      double wj[C];
+    // projections of the later vectors, G x PV at a time: each group takes
+    // PV vectors per round, whose dot products and group sums are
+    // independent chains that overlap (a round is latency-bound: a 5-term
+    // FP64 dot product and three shuffle levels)
+    for (int j0 = q + 1; j0 < k; j0 += G * PV) {
+      double wj[PV][C], c[PV];
 #pragma unroll
-      for (int j = 0; j < C; j++) wj[j] = valid ? W[vj * N + li * C + j] : 0.0;
-      double c = 0;
+      for (int u = 0; u < PV; u++) {
+        const int vj = j0 + u * G + g;
+        const bool valid = vj < k;
 #pragma unroll
-      for (int j = 0; j < C; j++) c = fma(wq[j], wj[j], c);
-      c = group_sum(c);
-      if (valid)
+        for (int j = 0; j < C; j++) wj[u][j] = valid ? W[vj * N + li * C + j] : 0.0;
+        c[u] = 0.0;
 #pragma unroll
-        for (int j = 0; j < C; j++) W[vj * N + li * C + j] = fma(-c, wq[j], wj[j]);
+        for (int j = 0; j < C; j++) c[u] = fma(wq[j], wj[u][j], c[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < PV; u++) c[u] = group_sum(c[u]);
+#pragma unroll
+      for (int u = 0; u < PV; u++) {
+        const int vj = j0 + u * G + g;
+        if (vj < k)
+#pragma unroll
+          for (int j = 0; j < C; j++) W[vj * N + li * C + j] = fma(-c[u], wq[j], wj[u][j]);
+      }
     }
     __syncwarp();
     if (ok) {
