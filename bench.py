@@ -73,7 +73,9 @@ WORKLOADS = {
         precision="fp32", rtol=1e-6, atol=1e-6, h=1e-3, t_transient=100.0, t_avg=1000.0,
         dt_renorm=1.0, dtype="fp32", ref_h=1e-3,
         plain=dict(integrator="dverk65", precision="fp64", rtol=1e-10, atol=1e-10),
-        second="rossler1024"),
+        second="rossler1024",
+        # the other configurations, each timed once beside the headline (1 GPU)
+        configs=["lorenz64", "l96_256", "batch256"]),
     # warp-per-point form: Lorenz-96, N = 40, full 40-exponent spectrum
     "l96_256": dict(
         model="lorenz96", base=[8.0, 1.0], s1=[0, 4.0, 16.0, 256], s2=[1, 0.5, 1.5, 256],
@@ -398,6 +400,15 @@ def run_surrogate_bench(a, rank, world, local):
 def run_batch_bench(a, rank, world, local):
     """--workload batch256: the mixed batch through a CUDA graph, beside the
     same three sweeps launched one after another without the work queue."""
+    line = measure_batch(a, rank, world, local, a.steps, a.warmup, unbatched=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batch(a, rank, world, local, nsteps, nwarm, unbatched=True):
+    """The mixed batch (config 3) as a replayed graph: `nwarm` untimed and
+    `nsteps` timed replays; with `unbatched`, also the three sweeps launched in
+    turn.  Returns the bench line (meaningful on rank 0)."""
     import torch
     import torch.distributed as dist
     import chaos_oneapi_b200 as cl
@@ -433,7 +444,7 @@ def run_batch_bench(a, rank, world, local):
     peak = cl.fma_peak_tflops(local, "fp32", 1.0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     with torch.cuda.stream(stream):
-        for _ in range(a.warmup):
+        for _ in range(nwarm):
             graph.launch(stream)
         stream.synchronize()
         clocks = ClockSampler(local)
@@ -443,7 +454,7 @@ def run_batch_bench(a, rank, world, local):
         clocks.start()
         t0e, t1e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0e.record(stream)
-        for i in range(a.steps):
+        for i in range(nsteps):
             flush.fill_(i & 0xFF)
             graph.launch(stream)
         t1e.record(stream)
@@ -452,23 +463,26 @@ def run_batch_bench(a, rank, world, local):
             dist.barrier()
         clk = clocks.stop()
         elapsed_ms = t0e.elapsed_time(t1e)
-        # the same work without batching: three direct launches in a row
-        dev_ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(parts) + 1)]
-        dev_ev[0].record(stream)
-        for i, (sw_d, pt) in enumerate(zip(direct, parts)):
-            sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
-            dev_ev[i + 1].record(stream)
-        stream.synchronize()
-        direct_ms = dev_ev[0].elapsed_time(dev_ev[-1])
-        direct_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
-        # and the same three sweeps in the split form (four lanes per point)
-        dev_ev[0].record(stream)
-        for i, (sw_d, pt) in enumerate(zip(direct_split, parts)):
-            sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
-            dev_ev[i + 1].record(stream)
-        stream.synchronize()
-        split_ms = dev_ev[0].elapsed_time(dev_ev[-1])
-        split_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
+        direct_ms = split_ms = float("nan")
+        direct_seg_ms = split_seg_ms = []
+        if unbatched:
+            # the same work without batching: three direct launches in a row
+            dev_ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(parts) + 1)]
+            dev_ev[0].record(stream)
+            for i, (sw_d, pt) in enumerate(zip(direct, parts)):
+                sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
+                dev_ev[i + 1].record(stream)
+            stream.synchronize()
+            direct_ms = dev_ev[0].elapsed_time(dev_ev[-1])
+            direct_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
+            # and the same three sweeps in the split form (four lanes per point)
+            dev_ev[0].record(stream)
+            for i, (sw_d, pt) in enumerate(zip(direct_split, parts)):
+                sw_d.run(pt[1], pt[2], pt[3], pt[4], pt[5], t_avg=pt[6], stream=stream)
+                dev_ev[i + 1].record(stream)
+            stream.synchronize()
+            split_ms = dev_ev[0].elapsed_time(dev_ev[-1])
+            split_seg_ms = [dev_ev[i].elapsed_time(dev_ev[i + 1]) for i in range(len(parts))]
         # end to end: inputs from pinned host memory, results back, each step
         torch.cuda.synchronize(dev)
         e0 = time.perf_counter()
@@ -485,7 +499,7 @@ def run_batch_bench(a, rank, world, local):
         t = torch.tensor([elapsed_ms, direct_ms, e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms, direct_ms, e2e_s = t.tolist()
-    value = total_points * a.steps * world / (elapsed_ms * 1e-3)
+    value = total_points * nsteps * world / (elapsed_ms * 1e-3)
     fl, pts = 0.0, {}
     for (sw, p, x, spec, st, steps, tv) in parts:
         stp = steps.cpu().numpy()
@@ -495,40 +509,42 @@ def run_batch_bench(a, rank, world, local):
                              "escaped": int((stt == 4).sum()), "steps_mean": float(stp.mean()),
                              "steps_p99": float(np.percentile(stp, 99)),
                              "steps_max": int(stp.max())}
-    achieved = fl / (elapsed_ms / a.steps * 1e-3) / 1e12
+    achieved = fl / (elapsed_ms / nsteps * 1e-3) / 1e12
     h2d = sum(int(h.numel() * 8) for hs in host for h in hs)
     d2h = sum(int(o[0].numel() * 8 + o[1].numel() * 4) for o in outs)
     graph.close()
-    if rank == 0:
-        line = {
-            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": elapsed_ms / a.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic (seeded grids, jitter and averaging times)",
-            "config": {"workload": "batch256", "segments": list(BATCH),
-                       "grid_per_segment": (f"{a.grid}x{a.grid}" if a.grid > 0 else "256x256"),
-                       "points_per_step": total_points,
-                       "t_avg": (f"U[1000, 10000] x {a.t_scale:g} per point" if a.t_scale != 1.0
-                                 else "U[1000, 10000] per point"),
-                       **{k: v for k, v in BATCH_KW.items() if k != "t_avg"},
-                       "launch": "one persistent batch kernel per step, replayed CUDA graph",
-                       "form": {name: ("one point per group of four lanes"
-                                       if form_of(name).startswith("split") else
-                                       "one point per lane") for name in BATCH}},
-            "gpu_launches": a.steps, "clocks": clk,
-            "roofline": {"bound": "fp32_fma", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                         "peak_source": "measured in-process (FMA-chain kernel)"},
-            "unbatched": {"ms": direct_ms, "points_per_s": total_points / (direct_ms * 1e-3),
-                          "segment_ms": direct_seg_ms,
-                          "split_ms": split_ms, "split_segment_ms": split_seg_ms,
-                          "how": "the three sweeps launched in turn, no work queue: ms one "
-                                 "thread per point, split_ms one group of four lanes per point"},
-            "e2e": {"value": total_points * world / e2e_s, "unit": "points/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": 1},
-            "points": pts,
-        }
-        print(json.dumps(line), flush=True)
+    for sw in sweeps + direct + direct_split:
+        sw.close()
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+        "steps": nsteps, "warmup": nwarm, "ms_per_step": elapsed_ms / nsteps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded grids, jitter and averaging times)",
+        "config": {"workload": "batch256", "segments": list(BATCH),
+                   "grid_per_segment": (f"{a.grid}x{a.grid}" if a.grid > 0 else "256x256"),
+                   "points_per_step": total_points,
+                   "t_avg": (f"U[1000, 10000] x {a.t_scale:g} per point" if a.t_scale != 1.0
+                             else "U[1000, 10000] per point"),
+                   **{k: v for k, v in BATCH_KW.items() if k != "t_avg"},
+                   "launch": "one persistent batch kernel per step, replayed CUDA graph",
+                   "form": {name: ("one point per group of four lanes"
+                                   if form_of(name).startswith("split") else
+                                   "one point per lane") for name in BATCH}},
+        "gpu_launches": nsteps, "clocks": clk,
+        "roofline": {"bound": "fp32_fma", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured in-process (FMA-chain kernel)"},
+        "unbatched": ({"ms": direct_ms, "points_per_s": total_points / (direct_ms * 1e-3),
+                       "segment_ms": direct_seg_ms,
+                       "split_ms": split_ms, "split_segment_ms": split_seg_ms,
+                       "how": "the three sweeps launched in turn, no work queue: ms one "
+                              "thread per point, split_ms one group of four lanes per point"}
+                      if unbatched else None),
+        "e2e": {"value": total_points * world / e2e_s, "unit": "points/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": 1},
+        "points": pts,
+    }
+    return line
 
 
 def resident_mb(w):
@@ -799,6 +815,19 @@ def run_sweep_bench(a, w, rank, world, local):
     if a.with_rossler and w.get("second"):
         second = run_second_map(a, WORKLOADS[w["second"]], cl, torch, dev, stream, flush, local)
 
+    # the other configurations (64^2 FP64 map, Lorenz-96, mixed batch), each
+    # timed once after a warm run, so that one run records every one of them
+    configs = {}
+    if a.with_configs and world == 1:
+        for name in w.get("configs", []):
+            if name == "batch256":
+                configs[name] = measure_batch(a, 0, 1, local, nsteps=1, nwarm=1,
+                                              unbatched=False)
+            else:
+                configs[name] = run_second_map(a, WORKLOADS[name], cl, torch, dev, stream,
+                                               flush, local,
+                                               accuracy_sample=64 if name == "lorenz64" else 0)
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -876,6 +905,8 @@ def run_sweep_bench(a, w, rank, world, local):
                                                             plain["status"][idx], ref, rst)
     if second is not None:
         line["precision_form_" + w["second"]] = second
+    if configs:
+        line["other_configs"] = configs
 
     if not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -890,23 +921,26 @@ def run_sweep_bench(a, w, rank, world, local):
         dist.destroy_process_group()
 
 
-def run_second_map(a, w, cl, torch, dev, stream, flush, local):
+def run_second_map(a, w, cl, torch, dev, stream, flush, local, accuracy_sample=None):
     """One timed sweep of workload `w` (after the autotuner and a warm-up) and
     its accuracy against the FP64 oracle on a random sample of
-    --second-accuracy-sample cells, split by regime."""
+    --second-accuracy-sample cells (or `accuracy_sample`), split by regime."""
     params, inits = build_inputs(w, 0)
     P = params.shape[0]
     k = w.get("k", 3)
     sw = cl.Sweep(model=w["model"], method="var", integrator=w["integrator"],
                   precision=w["precision"], rtol=w["rtol"], atol=w["atol"], h=w["h"],
                   t_transient=w["t_transient"], t_avg=w["t_avg"], dt_renorm=w["dt_renorm"],
-                  k=k, device=local, schedule="persistent")
+                  gs=w.get("gs", "cgs"), k=k, device=local, schedule="persistent")
     dp = torch.from_numpy(params).to(dev)
     dx = torch.from_numpy(inits).to(dev)
     ds = torch.empty((P, k), dtype=torch.float64, device=dev)
     st = torch.empty(P, dtype=torch.int32, device=dev)
     steps = torch.empty(P, dtype=torch.int64, device=dev)
-    tuned = sw.autotune(dp, dx, sample=min(P, 1 << 17))
+    if k > 4:  # warp-per-point kernel: one shape
+        tuned = {"block": 256, "schedule": "persistent", "layout": "warp per point"}
+    else:
+        tuned = sw.autotune(dp, dx, sample=min(P, 1 << 17))
     with torch.cuda.stream(stream):
         sw.run(dp, dx, ds, st, steps, stream=stream)
         flush.fill_(0x33)
@@ -923,6 +957,7 @@ def run_second_map(a, w, cl, torch, dev, stream, flush, local):
     sw.close()
     out = {"workload": {key: w[key] for key in ("model", "integrator", "precision", "rtol",
                                                  "t_transient", "t_avg", "dt_renorm")},
+           "exponents": k,
            "grid": f"{int(w['s1'][3])}x{int(w['s2'][3])}", "launch": tuned,
            "ms": ms, "points_per_s": P / (ms * 1e-3),
            "roofline": {"achieved": fl / (ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
@@ -930,9 +965,15 @@ def run_second_map(a, w, cl, torch, dev, stream, flush, local):
            "points": {"ok": int((status_np == 0).sum()), "escaped": int((status_np == 4).sum()),
                       "steps_mean": float(steps_np.mean()),
                       "transient_steps_mean": float(steps_tr.mean())}}
-    if a.second_accuracy_sample > 0:
+    if w["model"] == "lorenz96":  # exact on every point: sum(lambda) = -N gamma
+        okp = status_np == 0
+        tr = np.abs(spec_np[okp].sum(1) + 40.0 * params[okp, 1])
+        out["trace_identity"] = {"points": int(okp.sum()), "median_abs": float(np.median(tr)),
+                                 "max_abs": float(tr.max())}
+    n_acc = a.second_accuracy_sample if accuracy_sample is None else accuracy_sample
+    if n_acc > 0:
         rng = np.random.default_rng(4321)
-        idx = rng.choice(P, a.second_accuracy_sample, replace=False)
+        idx = rng.choice(P, min(n_acc, P), replace=False)
         runs = oracle_runs(w, params, inits, k, idx, w["rtol"], w["integrator"])
         ref, rst = runs.pop("truth")
         out["accuracy"] = dict(vs="FP64 adaptive oracle, rtol=atol=1e-12 (CPU)",
@@ -948,16 +989,19 @@ def apply_overrides(a, w):
         w["s1"] = w["s1"][:3] + [a.grid]
         w["s2"] = w["s2"][:3] + [a.grid]
         w.pop("second", None)
+        w.pop("configs", None)
     if a.t_scale != 1.0:
         w["t_transient"] *= a.t_scale
         w["t_avg"] *= a.t_scale
         w.pop("second", None)
+        w.pop("configs", None)
     if a.form:
         integ, prec, rtol = a.form.split(",")
         w.update(integrator=integ, precision=prec, rtol=float(rtol), atol=float(rtol),
                  dtype=prec)
         w.pop("plain", None)
         w.pop("second", None)
+        w.pop("configs", None)
     return w
 
 
@@ -993,6 +1037,8 @@ def main():
     ap.add_argument("--dump", default="",
                     help="surrogate: write the held-out cells' predictions and truth (npz)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", dest="with_configs", action="store_false",
+                    help="skip the other configurations timed beside the default workload")
     ap.add_argument("--accuracy-sample", type=int, default=1024)
     ap.add_argument("--second-accuracy-sample", type=int, default=1024,
                     help="lorenz1024: cells of the Rossler 1024^2 map checked against the oracle")

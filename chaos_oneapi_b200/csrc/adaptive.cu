@@ -37,7 +37,7 @@ __device__ __forceinline__ int64_t next_point(const AdaptiveArgs &a) {
 // autotuner picks the variant.
 template <class M, int K, class R, int INTEG, int MINB>
 __global__ void __launch_bounds__(128, MINB) sweep_kernel(const AdaptiveArgs a) {
-  const Ctl c = make_ctl<R>(a);
+  const Ctl &c = a.ctl;
   Lane<M, K, R, INTEG> L;
   int64_t pt = a.queue ? next_point(a) : (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool active = pt < a.P;
@@ -82,7 +82,9 @@ int launch_mri(const AdaptiveArgs &a, int block, int persistent_blocks, int vari
   } else {
     grid = (unsigned)((a.P + block - 1) / block);
   }
-  kern<<<grid, block, 0, s>>>(a);
+  AdaptiveArgs ka = a;
+  ka.ctl = make_ctl<R>(a);
+  kern<<<grid, block, 0, s>>>(ka);
   return (int)cudaGetLastError();
 }
 
@@ -127,7 +129,7 @@ __device__ __forceinline__ bool batch_take(const BatchArgs &b, int seg, int64_t 
 template <class M, class R, int INTEG>
 __device__ __noinline__ void lane_segment(const BatchArgs &b, int seg, bool active, int64_t pt) {
   const AdaptiveArgs &a = b.seg[seg];
-  const Ctl c = make_ctl<R>(a);
+  const Ctl &c = a.ctl;
   Lane<M, M::N, R, INTEG> L;
   if (active) lane_start(L, a, pt);
   while (__any_sync(0xffffffffu, active)) {
@@ -197,7 +199,8 @@ int launch_batch(int integ, int prec, const BatchArgs &b, int block, cudaStream_
   const int64_t full = (int64_t)std::max(1, per_sm) * sms;
   const int64_t cap = std::max<int64_t>(1, (int64_t)(full * std::min(1.0, std::max(share, 0.0))));
   const int64_t grid = std::min<int64_t>(cap, (total + block - 1) / block);
-  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority, b);
+  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority,
+                                  with_ctl(b, prec));
 }
 
 int launch_adaptive(int model, int integ, int prec, const AdaptiveArgs &a, int block,

@@ -376,17 +376,41 @@ template <class R> CL_HD float renorm_spread_limit(float rtol) {
   return 0.3f * logf(1.0f / fmaxf(rtol, ulp));
 }
 
-struct Ctl {
-  float rtol, atol, tau;
-  double rtol64, atol64;  // the tolerances for the FP64 form's error norm
-  double hmax, hmin;
-  int64_t max_steps;
-  double escape;
-};
 template <class R> CL_HD typename CtlReal<R>::type ctl_rtol(const Ctl &c) { return c.rtol; }
 template <> CL_HD double ctl_rtol<double>(const Ctl &c) { return c.rtol64; }
 template <class R> CL_HD typename CtlReal<R>::type ctl_atol(const Ctl &c) { return c.atol; }
 template <> CL_HD double ctl_atol<double>(const Ctl &c) { return c.atol64; }
+
+// Float nearest to x in the direction of +inf / -inf / zero.
+CL_HD float float_ru(double x) {
+#ifdef __CUDA_ARCH__
+  return __double2float_ru(x);
+#else
+  float f = (float)x;
+  return (double)f < x ? nextafterf(f, INFINITY) : f;
+#endif
+}
+CL_HD float float_rd(double x) {
+#ifdef __CUDA_ARCH__
+  return __double2float_rd(x);
+#else
+  float f = (float)x;
+  return (double)f > x ? nextafterf(f, -INFINITY) : f;
+#endif
+}
+CL_HD float float_rz(double x) { return x >= 0.0 ? float_rd(x) : float_ru(x); }
+
+// h >= hmin and h > hmax for a step of either precision.
+CL_HD bool step_at_least_hmin(float h, const Ctl &c) { return h >= c.hmin32; }
+CL_HD bool step_at_least_hmin(double h, const Ctl &c) { return h >= c.hmin; }
+CL_HD bool step_above_hmax(float h, const Ctl &c) { return h > c.hmax32; }
+CL_HD bool step_above_hmax(double h, const Ctl &c) { return h > c.hmax; }
+
+// Time left in a phase as the step precision, never above the exact time
+// left (rounded toward zero), so that a step no longer than it never
+// passes the phase end.
+template <class R> CL_HD R time_left_as(double t) { return (R)t; }
+template <> CL_HD float time_left_as<float>(double t) { return float_rz(t); }
 
 // Controller arithmetic of either precision: base-2 logarithm and power.
 CL_HD float ctl_log2(float x) { return fast_log2f(x); }
@@ -445,7 +469,7 @@ CL_HD bool point_finite(const R (&p)[NP], const R (&x)[N]) {
 // chain was a fifth of a step's latency where a step is latency-bound.
 template <class R, int INTEG, bool EXACT = false>
 CL_HD bool control(typename CtlReal<R>::type err2_in, R h, typename CtlReal<R>::type &lfac_old,
-                   bool &reject, double hmax, R &hnew) {
+                   bool &reject, const Ctl &c, R &hnew) {
   using C = typename CtlReal<R>::type;
   using T = typename std::conditional<EXACT, C, float>::type;
   constexpr T beta = T(0.04);
@@ -461,7 +485,7 @@ CL_HD bool control(typename CtlReal<R>::type err2_in, R h, typename CtlReal<R>::
     lf = lf < log2_facc1 ? lf : log2_facc1;
     R hn = h * (R)ctl_exp2(-lf);
     lfac_old = (C)(lerr > log2_fac_min<T>() ? lerr : log2_fac_min<T>());
-    if ((double)hn > hmax) hn = (R)hmax;
+    if (step_above_hmax(hn, c)) hn = (R)c.hmax;
     if (reject && hn > h) hn = h;
     reject = false;
     hnew = hn;
@@ -503,21 +527,23 @@ struct Lane {
   typename CtlReal<R>::type lfac_old;  // log2 of the previous accepted step's error (>= log2 1e-4)
   int32_t phase;
   bool reject;
-  double t_phase, phase_len;  // time into the current phase, its length
-  float t_gs, L;              // time since the last Gram-Schmidt, its target
-  float rate_max;             // largest recent log-cancellation per unit time
-  double prod[K];             // product of the norms since the last log
+  double t_left;  // time left in the current phase
+  R t_left_r;     // the same in the step precision, rounded toward zero
+  float t_gs, L;  // time since the last Gram-Schmidt, its target
+  float rate_max; // largest recent log-cancellation per unit time
   int64_t steps;
 };
 
-// The part of a lane's state that a step does not touch -- the compensated
-// log-norm sums (read at the rare flushes of the norm products), the
-// averaging time and the point index (read at phase ends) -- lives in a
-// per-thread slot of shared memory instead of registers, which leaves the
-// registers to the step itself.  Blocks have at most kMaxLaneBlock threads.
+// The part of a lane's state that a step does not touch -- the products of
+// the norms (touched at renormalisations), the compensated log-norm sums
+// (read at the rare flushes of those products), the averaging time and the
+// point index (read at phase ends) -- lives in a per-thread slot of shared
+// memory instead of registers, which leaves the registers to the step
+// itself.  Blocks have at most kMaxLaneBlock threads.
 constexpr int kMaxLaneBlock = 128;
 struct Cold {
-  double sum[4], comp[4];  // Kahan-compensated sums of log-norms (k <= 4)
+  double prod[4];          // product of the norms since the last log (k <= 4)
+  double sum[4], comp[4];  // Kahan-compensated sums of log-norms
   double t_avg;
   int64_t pt;
 };
@@ -776,15 +802,15 @@ CL_HD void refresh_tangent_derivs(Lane<M, K, R, INTEG> &L) {
 
 // Moves the running norm products into the compensated log sums.
 template <class M, int K, class R, int INTEG>
-CL_HD void lane_flush_logs(Lane<M, K, R, INTEG> &L) {
+CL_HD void lane_flush_logs(Lane<M, K, R, INTEG> &) {
+  Cold &c = cold_slot();
 #pragma unroll
   for (int i = 0; i < K; i++) {  // Kahan-compensated sum of log-norms
-    Cold &c = cold_slot();
-    const double y = log(L.prod[i]) - c.comp[i];
+    const double y = log(c.prod[i]) - c.comp[i];
     const double s = c.sum[i] + y;
     c.comp[i] = (s - c.sum[i]) - y;
     c.sum[i] = s;
-    L.prod[i] = 1.0;
+    c.prod[i] = 1.0;
   }
 }
 
@@ -817,6 +843,12 @@ template <class R> CL_HD R tangent_init(int i, int j) {
 }
 
 template <class M, int K, class R, int INTEG>
+CL_HD void lane_set_phase_time(Lane<M, K, R, INTEG> &L, double len) {
+  L.t_left = len;
+  L.t_left_r = time_left_as<R>(len);
+}
+
+template <class M, int K, class R, int INTEG>
 CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
   constexpr int N = M::N;
 #pragma unroll
@@ -825,14 +857,13 @@ CL_HD void lane_start_tangent(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a) {
     for (int j = 0; j < N; j++) L.V[i][j] = tangent_init<R>(i, j);
   refresh_tangent_derivs(L);
   L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
-  L.t_phase = 0.0;
   L.t_gs = 0.f;
   if (a.t_align > 0) {
     L.phase = kAlign;
-    L.phase_len = a.t_align;
+    lane_set_phase_time(L, a.t_align);
   } else {
     L.phase = kAverage;
-    L.phase_len = cold_slot().t_avg;
+    lane_set_phase_time(L, cold_slot().t_avg);
   }
 }
 
@@ -855,7 +886,7 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
 #pragma unroll
   for (int i = 0; i < K; i++) {
     cs.sum[i] = cs.comp[i] = 0.0;
-    L.prod[i] = 1.0;
+    cs.prod[i] = 1.0;
   }
   // The tangent rows ride along in the packed transient pass; start them
   // from zero so that they stay finite until the alignment phase sets them.
@@ -866,8 +897,7 @@ CL_HD void lane_start(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, int64_t pt
   if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
   if (a.t_transient > 0) {
     L.phase = kTransient;
-    L.phase_len = a.t_transient;
-    L.t_phase = 0.0;
+    lane_set_phase_time(L, a.t_transient);
     L.t_gs = 0.f;
   } else {
     lane_start_tangent(L, a);
@@ -888,11 +918,12 @@ CL_HD bool lane_gram_schmidt(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, con
     // Norms multiply into a running FP64 product; its log joins the
     // compensated sum only when it nears the edge of the double range (and
     // at the end), so most renormalisations take no logarithm at all.
+    Cold &cs = cold_slot();
     bool flush = false;
 #pragma unroll
     for (int i = 0; i < K; i++) {
-      L.prod[i] *= r[i];
-      flush = flush || !(L.prod[i] < 1e150 && L.prod[i] > 1e-150);
+      cs.prod[i] *= r[i];
+      flush = flush || !(cs.prod[i] < 1e150 && cs.prod[i] > 1e-150);
     }
     if (flush) lane_flush_logs(L);
   }
@@ -921,13 +952,14 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
     lane_finish(L, a, 3);
     return kFinished;
   }
-  if (!((double)L.h >= c.hmin)) {  // also catches h == 0 and NaN
+  if (!step_at_least_hmin(L.h, c)) {  // also catches h == 0 and NaN
     lane_finish(L, a, 2);
     return kFinished;
   }
-  const double remaining = L.phase_len - L.t_phase;
-  const bool clamped = (double)L.h >= remaining;
-  const R h = clamped ? (R)remaining : L.h;
+  // A proposal that reaches the phase end lands on it (t_left_r is the time
+  // left rounded toward zero, so a step that is not clamped never passes it)
+  const bool clamped = L.h >= L.t_left_r;
+  const R h = clamped ? L.t_left_r : L.h;
   const bool joint = L.phase != kTransient;
   R x1[N], V1[K][N], kx1[N], kv1[K][N];
   L.steps++;
@@ -943,7 +975,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
     return kRunning;
   }
   R hnew;
-  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {
+  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c, hnew)) {
 #pragma unroll
     for (int j = 0; j < N; j++) {
       L.x[j] = x1[j];
@@ -959,7 +991,10 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
         }
     }
     if (!clamped || hnew < h) L.h = hnew;  // else keep the unclamped proposal
-    L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
+    if (!clamped) {
+      L.t_left -= (double)h;
+      L.t_left_r = time_left_as<R>(L.t_left);
+    }
     L.t_gs += (float)h;
     if (!state_inside(L.x, c.escape)) {
       lane_finish(L, a, 4);
@@ -974,8 +1009,7 @@ CL_HD int lane_step(Lane<M, K, R, INTEG> &L, const AdaptiveArgs &a, const Ctl &c
           return kFinished;
         }
         L.phase = kAverage;
-        L.phase_len = cold_slot().t_avg;
-        L.t_phase = 0.0;
+        lane_set_phase_time(L, cold_slot().t_avg);
       } else {
         const bool ok = lane_gram_schmidt(L, a, c);
         lane_finish(L, a, ok ? 0 : 1);
@@ -992,9 +1026,19 @@ template <class R>
 CL_HD Ctl make_ctl(const AdaptiveArgs &a) {
   // A step below 1e-12 (model time units) is never meaningful here; it also
   // stops a point whose controller collapsed the step to zero.
+  const double hmax = a.hmax > 0 ? a.hmax : 1e300, hmin = fmax(a.hmin, 1e-12);
   return Ctl{(float)a.rtol, (float)a.atol, renorm_spread_limit<R>((float)a.rtol), a.rtol, a.atol,
-             a.hmax > 0 ? a.hmax : 1e300, fmax(a.hmin, 1e-12), a.max_steps,
+             hmax, hmin, float_ru(hmin), float_rd(hmax), a.max_steps,
              a.escape > 0 ? a.escape : 1e4};
+}
+
+// A batch's arguments with every segment's limits filled in for the
+// batch's precision (host side, before the launch).
+inline BatchArgs with_ctl(const BatchArgs &b, int prec) {
+  BatchArgs out = b;
+  for (int i = 0; i < b.nseg; i++)
+    out.seg[i].ctl = prec == kFP32 ? make_ctl<float>(b.seg[i]) : make_ctl<double>(b.seg[i]);
+  return out;
 }
 
 // One point start to finish on one thread (the host form of the kernel

@@ -33,6 +33,23 @@ struct CompatArgs {
   int32_t *status;        // nullable: 0 ok, 1 non-finite spectrum
 };
 
+// Tolerances and limits of the adaptive forms in the forms the kernels use
+// them (adaptive.cuh: make_ctl).  The launchers fill AdaptiveArgs::ctl, so
+// that these loop-invariant values sit in the kernel's parameter space and
+// take no registers.
+struct Ctl {
+  float rtol, atol, tau;  // tau: renormalisation cancellation target
+  double rtol64, atol64;  // the tolerances for the FP64 form's error norm
+  double hmax, hmin;
+  // The step limits as floats, rounded so that a float step compares with
+  // them exactly as with the double limits: h >= hmin32 iff h >= hmin
+  // (rounded up), h > hmax32 iff h > hmax (rounded down).  The FP32 forms
+  // test their steps against these and convert nothing per step.
+  float hmin32, hmax32;
+  int64_t max_steps;
+  double escape;
+};
+
 // Adaptive forms (DVERK 6(5) or Dopri5; FP64 or FP32 state and tangent; FP64
 // Gram-Schmidt and compensated log-norm sums).
 struct AdaptiveArgs {
@@ -52,6 +69,7 @@ struct AdaptiveArgs {
   unsigned long long *queue;  // nullable unless the launch is persistent
   uint64_t queue_stride;      // coprime to P: hand-out order q -> q * stride mod P
   const int32_t *order;       // nullable: hand-out order q -> order[q] (overrides the stride)
+  Ctl ctl;                    // set by the launchers from the fields above
 };
 
 // Longest-first hand-out order (order.cu): order = a permutation of [0, P)

@@ -27,7 +27,7 @@ __device__ __forceinline__ int64_t group_next_point(const AdaptiveArgs &a, const
 template <class M, class R, int INTEG, bool XCH>
 __global__ void __launch_bounds__(128) split_kernel(const AdaptiveArgs a) {
   const Group g = group_of();
-  const Ctl c = make_ctl<R>(a);
+  const Ctl &c = a.ctl;
   SplitLane<M, R, INTEG, XCH> L;
   int64_t pt = a.queue ? group_next_point(a, g)
                        : ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kSplitLanes;
@@ -73,7 +73,9 @@ int launch_split_mri(const AdaptiveArgs &a, int block, int variant, cudaStream_t
   } else {
     grid = (unsigned)need;
   }
-  kern<<<grid, block, 0, s>>>(a);
+  AdaptiveArgs ka = a;
+  ka.ctl = make_ctl<R>(a);
+  kern<<<grid, block, 0, s>>>(ka);
   return (int)cudaGetLastError();
 }
 
@@ -117,7 +119,7 @@ template <class M, class R, int INTEG>
 __device__ __noinline__ void split_segment(const BatchArgs &b, int seg, const Group &g, bool active,
                               int64_t pt) {
   const AdaptiveArgs &a = b.seg[seg];
-  const Ctl c = make_ctl<R>(a);
+  const Ctl &c = a.ctl;
   SplitLane<M, R, INTEG> L;
   if (active) split_start(L, a, pt, g);
   while (__any_sync(0xffffffffu, active)) {
@@ -204,7 +206,8 @@ int launch_batch_split(int integ, int prec, const BatchArgs &b, int block, cudaS
   const int64_t full = (int64_t)std::max(1, per_sm) * sms;
   const int64_t cap = std::max<int64_t>(1, (int64_t)(full * std::min(1.0, std::max(share, 0.0))));
   const int64_t grid = std::min<int64_t>(cap, (total + groups - 1) / groups);
-  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority, b);
+  return (int)launch_with_priority(kern, (unsigned)grid, (unsigned)block, s, high_priority,
+                                  with_ctl(b, prec));
 }
 
 }  // namespace chaos

@@ -100,7 +100,8 @@ struct SplitLane {
   typename CtlReal<R>::type lfac_old;
   int32_t phase;
   bool reject;
-  double t_phase, phase_len;
+  double t_left;  // time left in the current phase
+  R t_left_r;     // the same in the step precision, rounded toward zero
   float t_gs, L, rate_max;
   double prod;    // product of this vector's norms since the last log
   int64_t steps;
@@ -133,6 +134,12 @@ __device__ void split_finish(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs 
 }
 
 template <class M, class R, int INTEG, bool XCH>
+__device__ __forceinline__ void split_set_phase_time(SplitLane<M, R, INTEG, XCH> &L, double len) {
+  L.t_left = len;
+  L.t_left_r = time_left_as<R>(len);
+}
+
+template <class M, class R, int INTEG, bool XCH>
 __device__ void split_start_tangent(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
                                     const Group &g) {
   constexpr int N = M::N;
@@ -143,14 +150,13 @@ __device__ void split_start_tangent(SplitLane<M, R, INTEG, XCH> &L, const Adapti
   }
   if (INTEG == kDopri5) M::jv(L.v, L.kv, L.p, L.x);
   L.lfac_old = log2_fac_min<typename CtlReal<R>::type>();
-  L.t_phase = 0.0;
   L.t_gs = 0.f;
   if (a.t_align > 0) {
     L.phase = kAlign;
-    L.phase_len = a.t_align;
+    split_set_phase_time(L, a.t_align);
   } else {
     L.phase = kAverage;
-    L.phase_len = cold_slot().t_avg;
+    split_set_phase_time(L, cold_slot().t_avg);
   }
 }
 
@@ -178,8 +184,7 @@ __device__ void split_start(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &
   if (INTEG == kDopri5) M::f(L.x, L.kx, L.p);
   if (a.t_transient > 0) {
     L.phase = kTransient;
-    L.phase_len = a.t_transient;
-    L.t_phase = 0.0;
+    split_set_phase_time(L, a.t_transient);
     L.t_gs = 0.f;
   } else {
     split_start_tangent(L, a, g);
@@ -361,13 +366,12 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
     split_finish(L, a, g, 3);
     return kFinished;
   }
-  if (!((double)L.h >= c.hmin)) {
+  if (!step_at_least_hmin(L.h, c)) {
     split_finish(L, a, g, 2);
     return kFinished;
   }
-  const double remaining = L.phase_len - L.t_phase;
-  const bool clamped = (double)L.h >= remaining;
-  const R h = clamped ? (R)remaining : L.h;
+  const bool clamped = L.h >= L.t_left_r;  // as the one-lane form
+  const R h = clamped ? L.t_left_r : L.h;
   const bool joint = L.phase != kTransient;
   const int vi = vec_of<XCH>(g);
   const bool has_vec = vi >= 0 && vi < M::N;  // launches take k == dim
@@ -385,7 +389,7 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
     return kRunning;
   }
   R hnew;
-  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c.hmax, hnew)) {
+  if (control<R, INTEG>(err2, h, L.lfac_old, L.reject, c, hnew)) {
 #pragma unroll
     for (int j = 0; j < N; j++) {
       L.x[j] = x1[j];
@@ -399,7 +403,10 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
       }
     }
     if (!clamped || hnew < h) L.h = hnew;
-    L.t_phase = clamped ? L.phase_len : L.t_phase + (double)h;
+    if (!clamped) {
+      L.t_left -= (double)h;
+      L.t_left_r = time_left_as<R>(L.t_left);
+    }
     L.t_gs += (float)h;
     if (!state_inside(L.x, c.escape)) {
       split_finish(L, a, g, 4);
@@ -414,8 +421,7 @@ __device__ int split_step(SplitLane<M, R, INTEG, XCH> &L, const AdaptiveArgs &a,
           return kFinished;
         }
         L.phase = kAverage;
-        L.phase_len = cold_slot().t_avg;
-        L.t_phase = 0.0;
+        split_set_phase_time(L, cold_slot().t_avg);
       } else {
         const bool ok = split_gram_schmidt(L, a, c, g);
         split_finish(L, a, g, ok ? 0 : 1);

@@ -71,7 +71,7 @@ CL_HD void run_trajectory(const TrajectoryArgs &ta, int64_t pt) {
       continue;
     }
     R hnew;
-    const bool accepted = control<R, INTEG, true>(err2, h, L.lfac_old, L.reject, c.hmax, hnew);
+    const bool accepted = control<R, INTEG, true>(err2, h, L.lfac_old, L.reject, c, hnew);
     L.h = hnew;
     if (!accepted) continue;
     bool inside = true;
