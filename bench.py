@@ -11,7 +11,10 @@ transient 100, averaging 1000, renormalisation every 1), with the plain
 FP64 DVERK 6(5) rtol 1e-10 sweep of the same map timed once in the same
 run (the time ratio is the precision form's target), both forms' errors
 against the FP64 rtol 1e-12 oracle on 1024 random cells, and the Rossler
-map below timed once beside it with its own accuracy sample.
+map below timed once beside it with its own accuracy sample.  On one GPU the
+same line also carries the other configurations, each timed once after a
+warm run (``other_configs``): the 64 x 64 FP64 map (``lorenz64``), Lorenz-96
+(``l96_256``) and the mixed batch (``batch256``); --no-configs skips them.
 
 ``rossler1024`` (the precision form's configuration): Rossler
 dx = -y - z, dy = x + a y, dz = b + z (x - c), b = 0.2, on a 1024 x 1024 grid

@@ -156,6 +156,35 @@ CL_HD E lin(double c, E k, Rest... rest) {
   }
 }
 
+// Step-scaled combinations: acc + (h c1) k1 + (h c2) k2 + ... (left to
+// right), one multiply-add per term.  The products h c are formed once per
+// pass (scalars, shared by every row), so a stage argument y + h sum a k
+// costs one instruction per term instead of one more for the final h, and
+// its last term -- the derivative just computed -- is one dependent
+// multiply-add away from the argument instead of two.
+template <class S, class E> CL_HD E linh(S, E acc) { return acc; }
+template <class S, class E, class... Rest>
+CL_HD E linh(S h, E acc, double c, E k, Rest... rest) {
+  return linh<S, E>(h, vfma(h * S(c), k, acc), rest...);
+}
+// The same without a starting value: (h c1) k1 + (h c2) k2 + ...
+template <class S, class E, class... Rest>
+CL_HD E linh0(S h, double c, E k, Rest... rest) {
+  return linh<S, E>(h, vmul(h * S(c), k), rest...);
+}
+// Which element types combine their stages step-scaled (FoldH) rather than
+// as y + h (sum a k), the reference's order (cuda/tools/dopri.dp.cpp:54-63).
+// The passes keep the reference's order when HF is false: in the trajectory
+// kernel, whose step sequence is compared with the reference's, and for
+// single FP64 rows -- the one-lane FP64 sweep, which is bound by FP64
+// throughput and forms the products once per row pass (4 passes per step),
+// measured 2.6 % slower step-scaled.  The packed FP32 rows (FMA-pipe bound,
+// 1 % faster) and the FP64 pairs and exchange rows of the four-lane form
+// (latency-bound: one dependent FP64 operation less per stage, 7 % faster
+// on the 64^2 map) fold.
+template <class E> struct FoldH { static constexpr bool value = true; };
+template <> struct FoldH<double> { static constexpr bool value = false; };
+
 // Arithmetic of the error norm and the step-size controller: FP32 for the
 // FP32 form, FP64 for the FP64 form.
 template <class R> struct CtlReal { using type = float; };
@@ -174,12 +203,14 @@ CL_HD void err_acc(float y0, float y1, float e, float rtol, float atol, float &a
   const float r = fast_div(e, fmaf(rtol, m, atol));
   acc = fmaf(r, r, acc);
 }
-// The pair shares one reciprocal: 1 / (s_x s_y) scaled by the other weight.
+// A packed pair of rows: both weights in one FFMA2, one hardware reciprocal
+// each (XU pipe), the weighted errors and their squares in FFMA2 / FMUL2.
+// The kernel is bound by the FMA pipe, so the XU takes the reciprocals
+// rather than the FMA pipe taking the scalings of a shared one.
 CL_HD void err_acc(float2 y0, float2 y1, float2 e, float rtol, float atol, float2 &acc) {
-  const float sx = fmaf(rtol, fmaxf(fabsf(y0.x), fabsf(y1.x)), atol);
-  const float sy = fmaf(rtol, fmaxf(fabsf(y0.y), fabsf(y1.y)), atol);
-  const float inv = fast_div(1.0f, sx * sy);
-  const float2 r = vmul2(e, make_float2(sy * inv, sx * inv));
+  const float2 m = make_float2(fmaxf(fabsf(y0.x), fabsf(y1.x)), fmaxf(fabsf(y0.y), fabsf(y1.y)));
+  const float2 sc = vfma2(make_float2(rtol, rtol), m, make_float2(atol, atol));
+  const float2 r = vmul2(e, make_float2(fast_div(1.0f, sc.x), fast_div(1.0f, sc.y)));
   acc = vfma2(r, r, acc);
 }
 CL_HD double recip(double x) {
@@ -230,111 +261,203 @@ CL_HD void err_row(const E *y0, const E *y1, const E *he, T rtol, T atol, A &acc
 // One DVERK 6(5) pass over an N-vector y of elements E: y1 = 6th-order
 // solution, err2 += squared weighted error components.  fn(s, arg, out)
 // evaluates the derivative of stage s (0-based) at arg.
-template <int N, class E, class F>
+template <int N, class E, class F, bool HF = FoldH<E>::value>
 CL_HD void dverk_pass(const E *y, typename ScalarOf<E>::type h, const F &fn, E *y1,
                       typename ErrAcc<E>::type &err2,
                       typename CtlReal<typename ScalarOf<E>::type>::type rtol,
                       typename CtlReal<typename ScalarOf<E>::type>::type atol) {
   using S = typename ScalarOf<E>::type;
   using T = DV;
-  E k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
-  fn(0, y, k1);
+  if constexpr (HF) {
+    E k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
+    fn(0, y, k1);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
-  fn(1, arg, k2);
+    for (int j = 0; j < N; j++) arg[j] = linh<S>(h, y[j], T::a21, k1[j]);
+    fn(1, arg, k2);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
-  fn(2, arg, k3);
+    for (int j = 0; j < N; j++) arg[j] = linh<S>(h, y[j], T::a31, k1[j], T::a32, k2[j]);
+    fn(2, arg, k3);
 #pragma unroll
-  for (int j = 0; j < N; j++)
-    arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
-  fn(3, arg, k4);
+    for (int j = 0; j < N; j++)
+      arg[j] = linh<S>(h, y[j], T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]);
+    fn(3, arg, k4);
 #pragma unroll
-  for (int j = 0; j < N; j++)
-    arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
-  fn(4, arg, k5);
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
-                            T::a65, k5[j]), y[j]);
-    acc[j] = lin<S>(T::b1, k1[j], T::b3, k3[j], T::b4, k4[j], T::b5, k5[j]);
-    e[j] = lin<S>(T::d1, k1[j], T::d3, k3[j], T::d4, k4[j], T::d5, k5[j]);
-  }
-  {
-    E k6[N];
-    fn(5, arg, k6);
-#pragma unroll
-    for (int j = 0; j < N; j++) e[j] = vfma(S(T::d6), k6[j], e[j]);
-  }
-#pragma unroll
-  for (int j = 0; j < N; j++)
-    arg[j] = vfma(h, lin<S>(T::a71, k1[j], T::a72, k2[j], T::a73, k3[j], T::a74, k4[j],
-                            T::a75, k5[j]), y[j]);
-  fn(6, arg, k7);
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    arg[j] = vfma(h, lin<S>(T::a81, k1[j], T::a82, k2[j], T::a83, k3[j], T::a84, k4[j],
-                            T::a85, k5[j], T::a87, k7[j]), y[j]);
-    acc[j] = vfma(S(T::b7), k7[j], acc[j]);
-    e[j] = vfma(S(T::d7), k7[j], e[j]);
-  }
-  {
-    E k8[N];
-    fn(7, arg, k8);
+    for (int j = 0; j < N; j++)
+      arg[j] = linh<S>(h, y[j], T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]);
+    fn(4, arg, k5);
 #pragma unroll
     for (int j = 0; j < N; j++) {
-      acc[j] = vfma(S(T::b8), k8[j], acc[j]);
-      e[j] = vmul(h, vfma(S(T::d8), k8[j], e[j]));
-      y1[j] = vfma(h, acc[j], y[j]);
+      arg[j] = linh<S>(h, y[j], T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                       T::a65, k5[j]);
+      acc[j] = linh<S>(h, y[j], T::b1, k1[j], T::b3, k3[j], T::b4, k4[j], T::b5, k5[j]);
+      e[j] = linh0<S>(h, T::d1, k1[j], T::d3, k3[j], T::d4, k4[j], T::d5, k5[j]);
     }
+    {
+      E k6[N];
+      fn(5, arg, k6);
+#pragma unroll
+      for (int j = 0; j < N; j++) e[j] = linh<S>(h, e[j], T::d6, k6[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = linh<S>(h, y[j], T::a71, k1[j], T::a72, k2[j], T::a73, k3[j], T::a74, k4[j],
+                       T::a75, k5[j]);
+    fn(6, arg, k7);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      arg[j] = linh<S>(h, y[j], T::a81, k1[j], T::a82, k2[j], T::a83, k3[j], T::a84, k4[j],
+                       T::a85, k5[j], T::a87, k7[j]);
+      acc[j] = linh<S>(h, acc[j], T::b7, k7[j]);
+      e[j] = linh<S>(h, e[j], T::d7, k7[j]);
+    }
+    {
+      E k8[N];
+      fn(7, arg, k8);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        y1[j] = linh<S>(h, acc[j], T::b8, k8[j]);
+        e[j] = linh<S>(h, e[j], T::d8, k8[j]);
+      }
+    }
+    err_row<N>(y, y1, e, rtol, atol, err2);
+  } else {
+    E k1[N], k2[N], k3[N], k4[N], k5[N], k7[N], arg[N], acc[N], e[N];
+    fn(0, y, k1);
+#pragma unroll
+    for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
+    fn(1, arg, k2);
+#pragma unroll
+    for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
+    fn(2, arg, k3);
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
+    fn(3, arg, k4);
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
+    fn(4, arg, k5);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                              T::a65, k5[j]), y[j]);
+      acc[j] = lin<S>(T::b1, k1[j], T::b3, k3[j], T::b4, k4[j], T::b5, k5[j]);
+      e[j] = lin<S>(T::d1, k1[j], T::d3, k3[j], T::d4, k4[j], T::d5, k5[j]);
+    }
+    {
+      E k6[N];
+      fn(5, arg, k6);
+#pragma unroll
+      for (int j = 0; j < N; j++) e[j] = vfma(S(T::d6), k6[j], e[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = vfma(h, lin<S>(T::a71, k1[j], T::a72, k2[j], T::a73, k3[j], T::a74, k4[j],
+                              T::a75, k5[j]), y[j]);
+    fn(6, arg, k7);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      arg[j] = vfma(h, lin<S>(T::a81, k1[j], T::a82, k2[j], T::a83, k3[j], T::a84, k4[j],
+                              T::a85, k5[j], T::a87, k7[j]), y[j]);
+      acc[j] = vfma(S(T::b7), k7[j], acc[j]);
+      e[j] = vfma(S(T::d7), k7[j], e[j]);
+    }
+    {
+      E k8[N];
+      fn(7, arg, k8);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        acc[j] = vfma(S(T::b8), k8[j], acc[j]);
+        e[j] = vmul(h, vfma(S(T::d8), k8[j], e[j]));
+        y1[j] = vfma(h, acc[j], y[j]);
+      }
+    }
+    err_row<N>(y, y1, e, rtol, atol, err2);
   }
-  err_row<N>(y, y1, e, rtol, atol, err2);
 }
 
 // One Dopri5 pass: k1 = derivative at y (FSAL, given), y1 = 5th-order
 // solution, k7 = derivative at y1 (the next step's k1).
-template <int N, class E, class F>
+template <int N, class E, class F, bool HF = FoldH<E>::value>
 CL_HD void dopri_pass(const E *y, const E *k1, typename ScalarOf<E>::type h, const F &fn,
                       E *y1, E *k7, typename ErrAcc<E>::type &err2,
                       typename CtlReal<typename ScalarOf<E>::type>::type rtol,
                       typename CtlReal<typename ScalarOf<E>::type>::type atol) {
   using S = typename ScalarOf<E>::type;
   using T = DP;
-  E k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
+  if constexpr (HF) {
+    E k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
-  fn(1, arg, k2);
+    for (int j = 0; j < N; j++) arg[j] = linh<S>(h, y[j], T::a21, k1[j]);
+    fn(1, arg, k2);
 #pragma unroll
-  for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
-  fn(2, arg, k3);
+    for (int j = 0; j < N; j++) arg[j] = linh<S>(h, y[j], T::a31, k1[j], T::a32, k2[j]);
+    fn(2, arg, k3);
 #pragma unroll
-  for (int j = 0; j < N; j++)
-    arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
-  fn(3, arg, k4);
+    for (int j = 0; j < N; j++)
+      arg[j] = linh<S>(h, y[j], T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]);
+    fn(3, arg, k4);
 #pragma unroll
-  for (int j = 0; j < N; j++)
-    arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
-  fn(4, arg, k5);
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
-                            T::a65, k5[j]), y[j]);
-    e[j] = lin<S>(T::e1, k1[j], T::e3, k3[j], T::e4, k4[j], T::e5, k5[j]);
-    y1[j] = lin<S>(T::a71, k1[j], T::a73, k3[j], T::a74, k4[j], T::a75, k5[j]);
-  }
-  {
-    E k6[N];
-    fn(5, arg, k6);
+    for (int j = 0; j < N; j++)
+      arg[j] = linh<S>(h, y[j], T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]);
+    fn(4, arg, k5);
 #pragma unroll
     for (int j = 0; j < N; j++) {
-      y1[j] = vfma(h, vfma(S(T::a76), k6[j], y1[j]), y[j]);
-      e[j] = vfma(S(T::e6), k6[j], e[j]);
+      arg[j] = linh<S>(h, y[j], T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                       T::a65, k5[j]);
+      e[j] = linh0<S>(h, T::e1, k1[j], T::e3, k3[j], T::e4, k4[j], T::e5, k5[j]);
+      y1[j] = linh<S>(h, y[j], T::a71, k1[j], T::a73, k3[j], T::a74, k4[j], T::a75, k5[j]);
     }
-  }
-  fn(6, y1, k7);
+    {
+      E k6[N];
+      fn(5, arg, k6);
 #pragma unroll
-  for (int j = 0; j < N; j++) e[j] = vmul(h, vfma(S(T::e7), k7[j], e[j]));
-  err_row<N>(y, y1, e, rtol, atol, err2);
+      for (int j = 0; j < N; j++) {
+        y1[j] = linh<S>(h, y1[j], T::a76, k6[j]);
+        e[j] = linh<S>(h, e[j], T::e6, k6[j]);
+      }
+    }
+    fn(6, y1, k7);
+#pragma unroll
+    for (int j = 0; j < N; j++) e[j] = linh<S>(h, e[j], T::e7, k7[j]);
+    err_row<N>(y, y1, e, rtol, atol, err2);
+  } else {
+    E k2[N], k3[N], k4[N], k5[N], arg[N], e[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a21, k1[j]), y[j]);
+    fn(1, arg, k2);
+#pragma unroll
+    for (int j = 0; j < N; j++) arg[j] = vfma(h, lin<S>(T::a31, k1[j], T::a32, k2[j]), y[j]);
+    fn(2, arg, k3);
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = vfma(h, lin<S>(T::a41, k1[j], T::a42, k2[j], T::a43, k3[j]), y[j]);
+    fn(3, arg, k4);
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      arg[j] = vfma(h, lin<S>(T::a51, k1[j], T::a52, k2[j], T::a53, k3[j], T::a54, k4[j]), y[j]);
+    fn(4, arg, k5);
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      arg[j] = vfma(h, lin<S>(T::a61, k1[j], T::a62, k2[j], T::a63, k3[j], T::a64, k4[j],
+                              T::a65, k5[j]), y[j]);
+      e[j] = lin<S>(T::e1, k1[j], T::e3, k3[j], T::e4, k4[j], T::e5, k5[j]);
+      y1[j] = lin<S>(T::a71, k1[j], T::a73, k3[j], T::a74, k4[j], T::a75, k5[j]);
+    }
+    {
+      E k6[N];
+      fn(5, arg, k6);
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        y1[j] = vfma(h, vfma(S(T::a76), k6[j], y1[j]), y[j]);
+        e[j] = vfma(S(T::e6), k6[j], e[j]);
+      }
+    }
+    fn(6, y1, k7);
+#pragma unroll
+    for (int j = 0; j < N; j++) e[j] = vmul(h, vfma(S(T::e7), k7[j], e[j]));
+    err_row<N>(y, y1, e, rtol, atol, err2);
+  }
 }
 
 // Stage evaluators for the state pass (records stage points) and the tangent
@@ -642,7 +765,7 @@ struct PairTangentStages {  // two tangent vectors at the recorded stage points
 
 // Attempt one step of length h; the tangent vectors only when `joint`.
 // Returns the mean square of the weighted error components (err^2).
-template <class M, int K, class R, int INTEG>
+template <class M, int K, class R, int INTEG, bool HF = FoldH<R>::value>
 CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, bool joint,
                                         typename CtlReal<R>::type rtol,
                                         typename CtlReal<R>::type atol, R (&x1)[M::N],
@@ -664,8 +787,8 @@ CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, boo
         ka[j] = make_float2(st.kx[j], st.kv[K - 1][j]);
       }
       PairStateStages<M> fa{st.p, X};
-      if (INTEG == kDverk65) dverk_pass<N, float2>(ya, h, fa, ya1, ea, rtol, atol);
-      else dopri_pass<N, float2>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
+      if (INTEG == kDverk65) dverk_pass<N, float2, decltype(fa), HF>(ya, h, fa, ya1, ea, rtol, atol);
+      else dopri_pass<N, float2, decltype(fa), HF>(ya, ka, h, fa, ya1, ka1, ea, rtol, atol);
 #pragma unroll
       for (int j = 0; j < N; j++) {
         x1[j] = ya1[j].x;
@@ -677,8 +800,8 @@ CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, boo
       }
     } else {
       StateStages<M, R> fs{st.p, X};
-      if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, ea.x, rtol, atol);
-      else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, ea.x, rtol, atol);
+      if (INTEG == kDverk65) dverk_pass<N, R, decltype(fs), HF>(st.x, h, fs, x1, ea.x, rtol, atol);
+      else dopri_pass<N, R, decltype(fs), HF>(st.x, st.kx, h, fs, x1, kx1, ea.x, rtol, atol);
     }
     float err2 = ea.x;
     if (joint) {
@@ -692,8 +815,8 @@ CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, boo
           yb[j] = make_float2(st.V[m][j], st.V[m + 1][j]);
           kb[j] = make_float2(st.kv[m][j], st.kv[m + 1][j]);
         }
-        if (INTEG == kDverk65) dverk_pass<N, float2>(yb, h, fb, yb1, eb, rtol, atol);
-        else dopri_pass<N, float2>(yb, kb, h, fb, yb1, kb1, eb, rtol, atol);
+        if (INTEG == kDverk65) dverk_pass<N, float2, decltype(fb), HF>(yb, h, fb, yb1, eb, rtol, atol);
+        else dopri_pass<N, float2, decltype(fb), HF>(yb, kb, h, fb, yb1, kb1, eb, rtol, atol);
 #pragma unroll
         for (int j = 0; j < N; j++) {
           V1[m][j] = yb1[j].x;
@@ -710,14 +833,14 @@ CL_HD typename CtlReal<R>::type attempt(const Lane<M, K, R, INTEG> &st, R h, boo
   } else {
     C err2 = C(0);
     StateStages<M, R> fs{st.p, X};
-    if (INTEG == kDverk65) dverk_pass<N, R>(st.x, h, fs, x1, err2, rtol, atol);
-    else dopri_pass<N, R>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
+    if (INTEG == kDverk65) dverk_pass<N, R, decltype(fs), HF>(st.x, h, fs, x1, err2, rtol, atol);
+    else dopri_pass<N, R, decltype(fs), HF>(st.x, st.kx, h, fs, x1, kx1, err2, rtol, atol);
     if (joint) {
       TangentStages<M, R> ft{st.p, st.x, X};
 #pragma unroll
       for (int i = 0; i < K; i++) {
-        if (INTEG == kDverk65) dverk_pass<N, R>(st.V[i], h, ft, V1[i], err2, rtol, atol);
-        else dopri_pass<N, R>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
+        if (INTEG == kDverk65) dverk_pass<N, R, decltype(ft), HF>(st.V[i], h, ft, V1[i], err2, rtol, atol);
+        else dopri_pass<N, R, decltype(ft), HF>(st.V[i], st.kv[i], h, ft, V1[i], kv1[i], err2, rtol, atol);
       }
     }
     return err2 * inv_nc;

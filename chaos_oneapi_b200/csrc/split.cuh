@@ -215,8 +215,10 @@ __device__ typename CtlReal<R>::type split_attempt(const SplitLane<M, R, INTEG, 
     }
     double er = 0.0;
     const ExchangeStages<M> fa{st.p, g.mask, g.base, state_lane};
-    if (INTEG == kDverk65) dverk_pass<N, double>(yr, h, fa, y1r, er, rtol, atol);
-    else dopri_pass<N, double>(yr, kr, h, fa, y1r, k1r, er, rtol, atol);
+    // step-scaled combinations (FoldH): the exchange rows are latency-bound
+    using FA = decltype(fa);
+    if (INTEG == kDverk65) dverk_pass<N, double, FA, true>(yr, h, fa, y1r, er, rtol, atol);
+    else dopri_pass<N, double, FA, true>(yr, kr, h, fa, y1r, k1r, er, rtol, atol);
 #pragma unroll
     for (int j = 0; j < N; j++) {
       x1[j] = __shfl_sync(g.mask, y1r[j], g.base);

@@ -8,7 +8,10 @@
 // the proposal and the state.  The step pass is the sweep kernels' own
 // (adaptive.cuh: attempt) and so is the controller, with its arithmetic in
 // FP64 for FP64 states (control<..., EXACT>; the sweeps evaluate it in
-// FP32).  DVERK 6(5) runs the same way with its own tableau and exponent.
+// FP32), and with the stage combinations in the reference's order y + h
+// (sum a k) (the FP32 sweeps and the four-lane forms fold h into the
+// coefficients instead; the FP64 one-lane sweep keeps this order).  DVERK
+// 6(5) runs the same way with its own tableau and exponent.
 #pragma once
 #include "adaptive.cuh"
 
@@ -59,8 +62,10 @@ CL_HD void run_trajectory(const TrajectoryArgs &ta, int64_t pt) {
     const R h = L.h;
     R x1[N], V1[K][N], kx1[N], kv1[K][N];
     L.steps++;
-    const C err2 = attempt<M, K, R, INTEG>(L, h, false, ctl_rtol<R>(c), ctl_atol<R>(c), x1, V1,
-                                           kx1, kv1);
+    // the reference's combination order (HF false): this step sequence is
+    // compared with the reference's dopriStep
+    const C err2 = attempt<M, K, R, INTEG, false>(L, h, false, ctl_rtol<R>(c), ctl_atol<R>(c),
+                                                  x1, V1, kx1, kv1);
     if (!(err2 <= err2_limit<C>())) {  // the sweeps' rule (point_finite)
       if (!point_finite(L.p, L.x)) {
         status = 1;
