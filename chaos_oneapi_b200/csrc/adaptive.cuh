@@ -174,16 +174,18 @@ CL_HD E linh0(S h, double c, E k, Rest... rest) {
 }
 // Which element types combine their stages step-scaled (FoldH) rather than
 // as y + h (sum a k), the reference's order (cuda/tools/dopri.dp.cpp:54-63).
-// The passes keep the reference's order when HF is false: in the trajectory
-// kernel, whose step sequence is compared with the reference's, and for
-// single FP64 rows -- the one-lane FP64 sweep, which is bound by FP64
-// throughput and forms the products once per row pass (4 passes per step),
-// measured 2.6 % slower step-scaled.  The packed FP32 rows (FMA-pipe bound,
-// 1 % faster) and the FP64 pairs and exchange rows of the four-lane form
-// (latency-bound: one dependent FP64 operation less per stage, 7 % faster
-// on the 64^2 map) fold.
-template <class E> struct FoldH { static constexpr bool value = true; };
-template <> struct FoldH<double> { static constexpr bool value = false; };
+// Only the FP64 pairs of the four-lane form (and its exchange rows, which
+// ask for it explicitly) fold: they are latency-bound, and each stage of
+// their serial chain loses one dependent FP64 operation (7 % on the 64^2
+// map).  Single FP64 rows -- the one-lane FP64 sweep, bound by FP64
+// throughput, which would form the products once per row pass -- measured
+// 2.6 % slower folded.  FP32 rows keep the reference's order as well: folded
+// they were 1 % faster, but the product h a rounded to FP32 at every step
+// moved one of the sensitive Rossler cells held at the full horizon from
+// within twice the FP64 method's error to 5x it.  The trajectory kernel,
+// whose step sequence is compared with the reference's, never folds.
+template <class E> struct FoldH { static constexpr bool value = false; };
+template <> struct FoldH<double2> { static constexpr bool value = true; };
 
 // Arithmetic of the error norm and the step-size controller: FP32 for the
 // FP32 form, FP64 for the FP64 form.

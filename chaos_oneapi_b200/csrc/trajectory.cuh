@@ -9,9 +9,9 @@
 // (adaptive.cuh: attempt) and so is the controller, with its arithmetic in
 // FP64 for FP64 states (control<..., EXACT>; the sweeps evaluate it in
 // FP32), and with the stage combinations in the reference's order y + h
-// (sum a k) (the FP32 sweeps and the four-lane forms fold h into the
-// coefficients instead; the FP64 one-lane sweep keeps this order).  DVERK
-// 6(5) runs the same way with its own tableau and exponent.
+// (sum a k), as in the one-lane sweeps (the four-lane FP64 forms fold h into
+// the coefficients instead).  DVERK 6(5) runs the same way with its own
+// tableau and exponent.
 #pragma once
 #include "adaptive.cuh"
 
