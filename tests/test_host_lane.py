@@ -135,3 +135,22 @@ def test_host_trajectory_follows_reference_dopri(traj_driver, name):
     assert int(out[0]) == 0
     rows = np.array([[float(v) for v in ln.split()] for ln in out[1:] if ln.strip()])
     tc.assert_follows_reference(rows[:, 0], rows[:, 1], rows[:, 2:], c)
+
+
+def test_float_step_limits_match_double_comparisons(tmp_path):
+    """The FP32 steps compare their proposals with the step limits as floats
+    and count the phase time down in float (adaptive.cuh: make_ctl,
+    step_at_least_hmin, step_above_hmax, time_left_as): for random limits and
+    the floats nearest them, every float comparison must answer as the
+    double comparison it replaces, and the float time left must be the
+    nearest float at or below the double time left."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not found")
+    out = str(tmp_path / "limits_driver")
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I" + os.path.join(ROOT, "include"), "-o", out,
+                    os.path.join(HERE, "host", "limits_driver.cu")], check=True,
+                   capture_output=True)
+    r = subprocess.run([out, "7", "20000"], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
