@@ -403,7 +403,7 @@ def run_surrogate_bench(a, rank, world, local):
 def run_batch_bench(a, rank, world, local):
     """--workload batch256: the mixed batch through a CUDA graph, beside the
     same three sweeps launched one after another without the work queue."""
-    line = measure_batch(a, rank, world, local, a.steps, a.warmup, unbatched=True)
+    line = measure_batch(a, rank, world, local, a.steps, a.warmup, unbatched=a.unbatched)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -1040,6 +1040,8 @@ def main():
     ap.add_argument("--dump", default="",
                     help="surrogate: write the held-out cells' predictions and truth (npz)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-unbatched", dest="unbatched", action="store_false",
+                    help="batch256: skip the three sweeps launched in turn")
     ap.add_argument("--no-configs", dest="with_configs", action="store_false",
                     help="skip the other configurations timed beside the default workload")
     ap.add_argument("--accuracy-sample", type=int, default=1024)

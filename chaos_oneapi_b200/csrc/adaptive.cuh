@@ -205,14 +205,12 @@ CL_HD void err_acc(float y0, float y1, float e, float rtol, float atol, float &a
   const float r = fast_div(e, fmaf(rtol, m, atol));
   acc = fmaf(r, r, acc);
 }
-// A packed pair of rows: both weights in one FFMA2, one hardware reciprocal
-// each (XU pipe), the weighted errors and their squares in FFMA2 / FMUL2.
-// The kernel is bound by the FMA pipe, so the XU takes the reciprocals
-// rather than the FMA pipe taking the scalings of a shared one.
+// The pair shares one reciprocal: 1 / (s_x s_y) scaled by the other weight.
 CL_HD void err_acc(float2 y0, float2 y1, float2 e, float rtol, float atol, float2 &acc) {
-  const float2 m = make_float2(fmaxf(fabsf(y0.x), fabsf(y1.x)), fmaxf(fabsf(y0.y), fabsf(y1.y)));
-  const float2 sc = vfma2(make_float2(rtol, rtol), m, make_float2(atol, atol));
-  const float2 r = vmul2(e, make_float2(fast_div(1.0f, sc.x), fast_div(1.0f, sc.y)));
+  const float sx = fmaf(rtol, fmaxf(fabsf(y0.x), fabsf(y1.x)), atol);
+  const float sy = fmaf(rtol, fmaxf(fabsf(y0.y), fabsf(y1.y)), atol);
+  const float inv = fast_div(1.0f, sx * sy);
+  const float2 r = vmul2(e, make_float2(sy * inv, sx * inv));
   acc = vfma2(r, r, acc);
 }
 CL_HD double recip(double x) {
