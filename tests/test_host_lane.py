@@ -154,3 +154,29 @@ def test_float_step_limits_match_double_comparisons(tmp_path):
                    capture_output=True)
     r = subprocess.run([out, "7", "20000"], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
+
+
+def test_step_scaled_combinations_are_the_same_method(tmp_path):
+    """The RK passes' step-scaled stage combinations, y + sum (h a) k (the
+    four-lane FP64 forms use them), against the reference's order y + h
+    (sum a k), on the same inputs (tests/host/fold_driver.cu): the new state
+    agrees to rounding and so does the error norm, for DVERK 6(5) and
+    Dopri5, single FP64 rows, FP64 pairs and packed FP32 pairs.  A
+    coefficient of one form mapped to another stage would move the state by
+    a part of the step's increment (~1e-2 relative here)."""
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not found")
+    out = str(tmp_path / "fold_driver")
+    subprocess.run([nvcc, "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I" + os.path.join(ROOT, "include"), "-o", out,
+                    os.path.join(HERE, "host", "fold_driver.cu")], check=True,
+                   capture_output=True)
+    lines = subprocess.run([out, "11", "12"], check=True, capture_output=True,
+                           text=True).stdout.split("\n")
+    rows = [ln.split() for ln in lines if ln.strip()]
+    assert len(rows) == 12 * 12
+    for integ, elem, model, dy, derr, norm in rows:
+        fp32 = elem == "fp32pair"
+        assert float(dy) <= (2e-6 if fp32 else 1e-14), (integ, elem, model, dy)
+        assert float(derr) <= (2e-3 if fp32 else 1e-9), (integ, elem, model, derr, norm)
