@@ -66,3 +66,20 @@ def test_reference_arm_inputs_come_from_the_oracle():
     p1, x1 = bench.build_inputs(w, 1, src=oracle)
     p2, x2 = bench.build_inputs(w, 1)
     assert np.array_equal(p1, p2) and np.array_equal(x1, x2)
+
+
+def test_default_line_names_every_other_configuration():
+    """The default line times the other configurations beside the headline
+    (64^2 FP64 map, Lorenz-96, mixed batch); a run that reshapes the
+    workload (--grid, --t-scale, --form) drops them with the second map."""
+    import argparse
+    w = bench.WORKLOADS["lorenz1024"]
+    assert w["configs"] == ["lorenz64", "l96_256", "batch256"]
+    for name in w["configs"]:
+        assert name in bench.WORKLOADS or name == "batch256"
+    for over in (dict(grid=64), dict(t_scale=0.1), dict(form="dopri5,fp32,1e-6")):
+        a = argparse.Namespace(grid=0, t_scale=1.0, form="")
+        for k, v in over.items():
+            setattr(a, k, v)
+        ww = bench.apply_overrides(a, dict(w))
+        assert "configs" not in ww and "second" not in ww, over
