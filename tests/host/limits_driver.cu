@@ -4,8 +4,10 @@
 // step_at_least_hmin, step_above_hmax, time_left_as, make_ctl).  For random
 // limits and random float steps near them, the float comparison must give
 // the same answer as the double comparison it replaces, and the phase time
-// left in float must never exceed the double time left.  Built by
-// tests/test_host_lane.py with nvcc; never linked into the library.
+// left in float must never exceed the double time left; and a batch's
+// launch arguments carry every segment's limits in the batch's precision
+// (with_ctl).  Built by tests/test_host_lane.py with nvcc; never linked into
+// the library.
 //
 //   limits_driver SEED N
 // Prints "ok CASES" or the first failing case.
@@ -63,6 +65,32 @@ int main(int argc, char **argv) {
     if (!((double)tr <= t) || !((double)nextafterf(tr, INFINITY) > t)) {
       printf("t %.17g: float %.9g\n", t, (double)tr);
       return 1;
+    }
+  }
+  // a batch's launch arguments: every segment gets the limits of its own
+  // fields in the batch's precision (with_ctl), the others stay untouched
+  BatchArgs b{};
+  b.nseg = 3;
+  for (int i = 0; i < kMaxSegments; i++) {
+    b.seg[i].rtol = b.seg[i].atol = 1e-6 * (i + 1);
+    b.seg[i].hmin = 1e-9 * (i + 1);
+    b.seg[i].hmax = 0.5 * (i + 1);
+    b.seg[i].max_steps = 1000 * (i + 1);
+    b.seg[i].dt_renorm = 1.0;
+  }
+  for (int prec : {(int)kFP32, (int)kFP64}) {
+    const BatchArgs w = with_ctl(b, prec);
+    for (int i = 0; i < kMaxSegments; i++) {
+      const Ctl want = i >= b.nseg ? Ctl{} : prec == kFP32 ? make_ctl<float>(b.seg[i])
+                                                           : make_ctl<double>(b.seg[i]);
+      const Ctl &got = w.seg[i].ctl;
+      ++cases;
+      if (got.rtol != want.rtol || got.tau != want.tau || got.hmin32 != want.hmin32 ||
+          got.hmax32 != want.hmax32 || got.hmin != want.hmin || got.hmax != want.hmax ||
+          got.max_steps != want.max_steps || got.escape != want.escape) {
+        printf("batch segment %d precision %d: limits not filled\n", i, prec);
+        return 1;
+      }
     }
   }
   printf("ok %ld\n", cases);
