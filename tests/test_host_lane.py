@@ -143,7 +143,9 @@ def test_float_step_limits_match_double_comparisons(tmp_path):
     step_at_least_hmin, step_above_hmax, time_left_as): for random limits and
     the floats nearest them, every float comparison must answer as the
     double comparison it replaces, and the float time left must be the
-    nearest float at or below the double time left."""
+    nearest float at or below the double time left.  A batch's launch
+    arguments must carry every segment's limits in the batch's precision
+    (with_ctl)."""
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(nvcc):
         pytest.skip("nvcc not found")
